@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the solid-mechanics Newton step on the 100^3 hex8 J2 mesh (3,090,903 DOFs).
+
+Metric (one JSON line on rank 0): hex8 elements assembled per second, where one assembly is the
+full fused pass that neon splits over update_internal_variables + assemble_stiffness +
+compute_internal_force: deformation measures, the J2 return mapping at all 8,000,000 quadrature
+points (plastic state), the tangent stiffness scattered into the 245,438,109-entry CSR pattern and
+the internal force.  A step = one assembly with inputs resident in HBM (K, state and pattern are
+far larger than L2, so no flush is needed).  Reported beside it: the Newton-step time of the
+FP64 and mixed-precision device paths on the first load increment of the cyclic history, and
+the relative displacement error of the mixed path against the FP64 path.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank runs an independent replica (the problem does not shard across GPUs);
+``value`` sums the ranks' elements over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "hex8 elements assembled/s + Newton-step s @3M DOF: mixed vs FP64 GPU, err<=1e-8"
+UNIT = "elements/s"
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def plastic_displacement(mesh, level=2.5e-3):
+    """A displacement field well past first yield: uniaxial z stretch with a shear twist."""
+    X = mesh.X
+    u = np.zeros(3 * mesh.num_nodes)
+    u[2::3] = level * X[:, 2]
+    u[0::3] = 0.3 * level * X[:, 2] * (X[:, 1] - 0.5)
+    u[1::3] = -0.3 * level * X[:, 2] * (X[:, 0] - 0.5)
+    return u
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_work(mesh_size, nnz, n_nodes, E, nqp, fp64=True):
+    """Canonical algorithmic work of one J2 hex8 assembly (bytes, flops): K written once,
+    connectivity, X, u, f_int, J2 state read (7 FP64) and written (7 FP64) per point; FLOPs
+    29,040 per element (geometry, symmetric block B^T D B, f_int) + 250 per point (J2)."""
+    kbytes = (8 if fp64 else 4) * nnz
+    nbytes = 32 * E + 24 * n_nodes + 8 * 3 * n_nodes + 8 * 3 * n_nodes + 112 * nqp
+    flops = (29040.0 + 8 * 250.0) * E
+    return kbytes + nbytes, flops
+
+
+def cpu_baseline_sample(threads=None, target_seconds=15.0):
+    """The oracle (C++/OpenMP restatement of neon's path) timed on this host: update +
+    assembly + internal force of a J2 hex8 mesh in the same plastic state, elements/s."""
+    from oracle import binding as ob
+    from neon_b200 import problem as P
+    if threads:
+        ob.set_threads(threads)
+    cores = ob.max_threads()
+
+    def run(n):
+        pr = P.config_c3(n)
+        om = ob.OracleMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+        u = plastic_displacement(pr.mesh)
+        t0 = time.perf_counter()
+        st, msg = om.update(u)
+        om.assemble()
+        om.internal_force()
+        dt = time.perf_counter() - t0
+        return pr.mesh.num_elements, dt
+
+    E0, t0 = run(20)
+    per_elem = t0 / E0
+    n = 20
+    for cand in (30, 40, 50, 60, 70, 80, 90, 100):
+        if cand ** 3 * per_elem * 1.3 <= target_seconds:
+            n = cand
+    E, dt = run(n)
+    reps = 1
+    total = dt
+    while total < target_seconds * 0.5 and reps < 5:
+        _, d2 = run(n)
+        total += d2
+        reps += 1
+    return {"value": E * reps / total, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle update+assembly+f_int of the J2 hex8 {n}^3 mesh ({E} elements, "
+                      f"plastic state) x{reps}, {cores} OpenMP threads"}
+
+
+def run_reference(args):
+    """Reference arm: the reference's CPU algorithm (oracle port; the reference itself cannot be
+    built here) on the same config, all host threads."""
+    rank = _env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    from oracle import binding as ob
+    from neon_b200 import problem as P
+    cores = ob.max_threads()
+    pr = P.config_c3(args.size)
+    om = ob.OracleMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+    u = plastic_displacement(pr.mesh)
+    E = pr.mesh.num_elements
+
+    def step():
+        om.save(False)  # revert to the committed (elastic) state: same return mapping each step
+        om.update(u)
+        om.assemble()
+        om.internal_force()
+
+    om.save(True)
+    t0 = time.perf_counter()
+    step()
+    one = time.perf_counter() - t0
+    # each step is bounded: keep the whole run within a few minutes
+    budget = 150.0
+    warm = max(0, min(args.warmup, int(budget / 4 / max(one, 1e-9))))
+    steps = max(1, min(args.steps, int(budget / max(one, 1e-9))))
+    for _ in range(warm):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = E * steps / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 1,
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * dt / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"J2 hex8 {args.size}^3 assembly (update + K + f_int)",
+                       "elements": E, "dofs": om.ndofs, "nnz": int(om.nnz)},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{steps} full assemblies of the {args.size}^3 mesh on "
+                                       f"{cores} OpenMP threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=100)
+    ap.add_argument("--newton-load-steps", type=int, default=1)
+    ap.add_argument("--no-newton", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from neon_b200 import api, build
+    from neon_b200 import problem as P
+    build.build()
+    warmup = max(3, args.warmup)
+
+    pr = P.config_c3(args.size)
+    mesh = api.SolidMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+    stream = torch.cuda.Stream()
+    mesh.set_stream(stream.cuda_stream)
+    E, nqp = pr.mesh.num_elements, mesh.nqp
+    u = plastic_displacement(pr.mesh)
+    mesh.save_internal_variables(True)  # committed state: zero plastic strain
+    mesh.set_displacement(u)
+
+    def assembly_step():
+        mesh.save_internal_variables(False)  # revert: every step runs the same return mapping
+        ev0.record(stream)
+        mesh.update_assemble_device(api.FP64)
+        ev1.record(stream)
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(warmup):
+        assembly_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    launches0 = mesh.launches()
+    kernel_ms = []
+    tw0 = torch.cuda.Event(enable_timing=True)
+    tw1 = torch.cuda.Event(enable_timing=True)
+    tw0.record(stream)
+    for _ in range(args.steps):
+        assembly_step()
+        ev1.synchronize()
+        kernel_ms.append(ev0.elapsed_time(ev1))
+    tw1.record(stream)
+    torch.cuda.synchronize()
+    launches = mesh.launches() - launches0
+    region_ms = tw0.elapsed_time(tw1)
+    clock_info = clocks.stop()
+    t_asm = sum(kernel_ms) / len(kernel_ms) * 1e-3
+    t_max = t_asm
+    if dist:
+        tt = torch.tensor([t_asm], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * E / t_max
+
+    # roofline of the dominant kernel (the fused element kernel)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    fp64_peak = api.probe_fma_throughput(True)
+    fp32_peak = api.probe_fma_throughput(False)
+    alg_bytes, alg_flops = algorithmic_work(args.size, mesh.nnz, pr.mesh.num_nodes, E, nqp)
+    t_hbm = alg_bytes / (hbm * 1e9)
+    t_fp = alg_flops / fp64_peak
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get("k_element_fp64_j2_hex8_bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+    if t_fp >= t_hbm:
+        roof = {"bound": "fp64", "achieved": alg_flops / t_asm / 1e12,
+                "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
+                "frac": (alg_flops / t_asm) / fp64_peak, "traffic": traffic,
+                "peak_source": "measured (FP64 FMA-chain probe, this run)",
+                "hbm": {"achieved": alg_bytes / t_asm / 1e9, "peak": hbm, "unit": "GB/s",
+                        "frac": (alg_bytes / t_asm / 1e9) / hbm, "peak_source": hbm_src},
+                "algorithmic_bytes": alg_bytes, "algorithmic_flops": alg_flops}
+    else:
+        roof = {"bound": "hbm", "achieved": alg_bytes / t_asm / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": (alg_bytes / t_asm / 1e9) / hbm, "traffic": traffic,
+                "peak_source": hbm_src, "algorithmic_bytes": alg_bytes,
+                "algorithmic_flops": alg_flops}
+
+    # end to end through the drop-in C-ABI with host buffers (copies inside the timed region)
+    mesh_e2e = api.SolidMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+    mesh_e2e.save_internal_variables(True)
+    Kh = np.zeros(mesh_e2e.nnz)
+    fh = np.zeros(mesh_e2e.ndofs)
+    import ctypes
+    L = api.lib()
+
+    def e2e_step():
+        mesh_e2e.save_internal_variables(False)
+        api._check(L.nb2_update_internal_variables(mesh_e2e.h, u.ctypes.data, 0.0), mesh_e2e.h)
+        api._check(L.nb2_assemble(mesh_e2e.h, Kh.ctypes.data, fh.ctypes.data), mesh_e2e.h)
+
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    t_e2e = (time.perf_counter() - t0) / args.e2e_steps
+    if dist:
+        tt = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = {"value": world * E / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * mesh_e2e.ndofs,
+           "d2h_bytes_per_step": 8 * mesh_e2e.nnz + 8 * mesh_e2e.ndofs,
+           "call": "nb2_update_internal_variables + nb2_assemble (host u in, host CSR K + f_int "
+                   "out)"}
+    mesh_e2e.close()
+
+    newton = None
+    if not args.no_newton:
+        newton = newton_comparison(api, P, args, mesh)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample()
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": warmup, "ms_per_step": t_max * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"J2 hex8 {args.size}^3 (sigma_y=200, E=200e3, nu=0.3, "
+                                   f"H=1e3), fused update+K+f_int, plastic state",
+                       "elements": E, "dofs": mesh.ndofs, "nnz": mesh.nnz,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (K 1.96 GB, state 0.45 GB)"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "timed_region_ms": region_ms, "clocks": clock_info,
+            "fp32_fma_peak_tflops": fp32_peak / 1e12, "newton": newton}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    mesh.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def newton_comparison(api, P, args, mesh_unused):
+    """FP64 vs mixed device Newton on the first load increment(s) of the cyclic J2 history."""
+    pr = P.config_c3(args.size)
+    pr.options.period = float(args.newton_load_steps)
+    out = {}
+    sols = {}
+    for name, prec, tol in (("fp64", api.FP64, None), ("mixed", api.MIXED, 1e-5)):
+        sm = api.StaticMatrix(pr, precision=prec, mixed_inner_tolerance=tol or 1e-6)
+        try:
+            u = sm.solve(raise_on_error=False)
+        finally:
+            sm.mesh.close()
+        r = sm.report
+        nit = max(1, int(r["newton_iterations"]))
+        sols[name] = u
+        out[name] = {"status": int(r["status"]), "load_steps": int(r["load_steps"]),
+                     "newton_iterations": int(r["newton_iterations"]),
+                     "cg_iterations": int(r["cg_iterations"]),
+                     "seconds_total": r["seconds_total"],
+                     "newton_step_s": r["seconds_total"] / nit,
+                     "device_s_elements": r["seconds_update_assembly"],
+                     "device_s_solve": r["seconds_solve"]}
+    u64, u32 = sols["fp64"], sols["mixed"]
+    out["mixed_rel_err_u"] = float(np.linalg.norm(u32 - u64) / max(np.linalg.norm(u64), 1e-300))
+    out["load_step_speedup"] = out["fp64"]["seconds_total"] / max(out["mixed"]["seconds_total"],
+                                                                  1e-12)
+    out["newton_step_speedup"] = out["fp64"]["newton_step_s"] / max(
+        out["mixed"]["newton_step_s"], 1e-12)
+    out["load_steps_run"] = args.newton_load_steps
+    return out
+
+
+if __name__ == "__main__":
+    sys.exit(main())

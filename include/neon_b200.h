@@ -1,0 +1,229 @@
+/* neon_b200.h -- C-ABI of the B200-native solid-mechanics Newton step.
+ *
+ * Drop-in for neon's nonlinear static solid path:
+ *   mechanics::static_matrix<mechanics::solid::mesh<solid::submesh>>
+ *     (src/assembler/mechanics/static_matrix.hpp:29-467),
+ *   its element kernels and internal-variable update
+ *     (src/mesh/mechanics/solid/submesh.cpp:66-269, mesh.cpp:56-76),
+ *   the constitutive plugins on the path
+ *     (src/constitutive/mechanics/solid/{isotropic_linear_elasticity,compressible_neohooke,
+ *      small_strain_J2_plasticity,gaussian_affine_microsphere}.cpp),
+ *   and the linear_solver plugin (src/solver/linear/linear_solver.hpp:13-71).
+ *
+ * Plain C types only.  Every call returns an nb2_status; nothing throws across the boundary.
+ * Host pointers are read (or written) only during the call.  A context is single-stream and not
+ * thread-safe; several contexts may run on several streams.
+ */
+#ifndef NEON_B200_H
+#define NEON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The recoverable numerical failures (1-6, 9) correspond to neon's
+ * computational_error (src/exceptions.hpp:14-17), which static_matrix::solve answers with a
+ * cutback (static_matrix.hpp:168-182).  NB2_E_INPUT corresponds to std::domain_error. */
+typedef enum nb2_status {
+    NB2_OK = 0,
+    NB2_E_NEG_DETJ = 1,      /* negative det F (submesh.cpp:239-269) */
+    NB2_E_NAN = 2,           /* FE_INVALID after an update / solve (submesh.cpp:196-207) */
+    NB2_E_RETURN_MAP = 3,    /* radial return did not converge (small_strain_J2_plasticity.cpp:132-153) */
+    NB2_E_CG_MAXIT = 4,      /* CG reached its iteration limit (linear_solver.cpp:104-108) */
+    NB2_E_CG_BREAKDOWN = 5,  /* CG denominator not positive / not finite */
+    NB2_E_TIMEOUT = 6,       /* a bounded device wait gave up */
+    NB2_E_INPUT = 7,         /* invalid argument */
+    NB2_E_CUDA = 8,          /* CUDA runtime error (message in nb2_last_error) */
+    NB2_E_NEWTON_MAXIT = 9,  /* Newton iteration limit (static_matrix.hpp:451-454) */
+    NB2_E_CUTBACK_LIMIT = 10 /* too many load cutbacks (adaptive_time_step.cpp:61-92) */
+} nb2_status;
+
+/* Constitutive models on the path (names as in constitutive_model_factory.cpp:26-161). */
+typedef enum nb2_model {
+    NB2_ISOTROPIC_LINEAR_ELASTICITY = 0, /* "isotropic_linear_elasticity" */
+    NB2_NEOHOOKE = 1,                    /* "neohooke" */
+    NB2_SMALL_STRAIN_J2_PLASTICITY = 2,  /* "J2_plasticity", "finite_strain": false */
+    NB2_GAUSSIAN_AFFINE_MICROSPHERE = 3  /* "microsphere", "affine", "gaussian", "BO21" */
+} nb2_model;
+
+/* Precision of the stiffness / inner linear solve. */
+typedef enum nb2_precision {
+    NB2_FP64 = 0,  /* everything FP64: parity path */
+    NB2_MIXED = 1  /* FP32 tangent, SpMV and inner CG; FP64 residual, norms, dots, return map, det F */
+} nb2_precision;
+
+typedef struct nb2_ctx nb2_ctx;
+
+/* Mesh: one element group (neon submesh).  Coordinates node-major [num_nodes][3]; DOF
+ * 3*node + component (mesh/dof_allocator.hpp:39-47).  Connectivity element-major
+ * [num_elements][nodes_per_element] in neon's local ordering (hex8: interpolations/hexahedron.cpp
+ * corner order; tet4 after node_ordering_adapter.cpp:63-68).  hex8 uses the 8-point Gauss rule,
+ * tet4 the 1-point rule (interpolation_factory.cpp:36-97). */
+typedef struct nb2_mesh_desc {
+    int32_t num_nodes;
+    const double* coordinates;
+    int32_t num_elements;
+    int32_t nodes_per_element; /* 8 (hex8) or 4 (tet4) */
+    const int32_t* connectivity;
+} nb2_mesh_desc;
+
+/* Material parameters as neon stores them: bulk modulus K and shear modulus G
+ * (isotropic_elastic_property.cpp:10-43, lambda = K - 2G/3), yield stress and linear isotropic
+ * hardening (isotropic_elastic_plastic.cpp:31-38), segments per chain
+ * (micromechanical_elastomer.cpp:13-21, required but unused by Gaussian statistics). */
+typedef struct nb2_material {
+    int32_t model; /* nb2_model */
+    double bulk_modulus;
+    double shear_modulus;
+    double yield_stress;
+    double isotropic_hardening_modulus;
+    double segments_per_chain;
+} nb2_material;
+
+/* A time/value table applied to a DOF list: a Dirichlet boundary (mesh/boundary/nodal_value.cpp,
+ * dirichlet.hpp) or a nodal force.  Values are interpolated linearly in time
+ * (mesh/boundary/boundary.cpp:55-85).  weights (nullable, forces only) scales the value per DOF:
+ * f_ext[dof[i]] += weights[i] * value(t). */
+typedef struct nb2_dof_table {
+    const int32_t* dofs;
+    int32_t num_dofs;
+    const double* times;
+    const double* values;
+    int32_t num_points;
+    const double* weights;
+} nb2_dof_table;
+
+/* nonlinear_options (static_matrix.hpp:109-143), time/increments (adaptive_time_step.cpp),
+ * linear_solver tolerance / maximum_iterations (linear_solver_factory.cpp:27-65). */
+typedef struct nb2_solver_options {
+    double residual_tolerance;
+    double displacement_tolerance;
+    int32_t linear_iterations; /* maximum Newton iterations per increment */
+    int32_t absolute_tolerance;
+    double period, initial_increment, minimum_increment, maximum_increment;
+    int32_t adaptive;
+    double cg_tolerance;
+    int32_t cg_maximum_iterations;
+    int32_t precision;         /* nb2_precision */
+    double mixed_inner_tolerance; /* NB2_MIXED: relative tolerance of each inner FP32 CG */
+    int32_t use_graphs;        /* capture CG iteration blocks in CUDA graphs */
+} nb2_solver_options;
+
+typedef struct nb2_solve_report {
+    int32_t status;
+    int32_t load_steps;
+    int64_t newton_iterations;
+    int64_t cg_iterations;
+    double seconds_total;
+    double seconds_update_assembly; /* device time of the element kernels */
+    double seconds_solve;           /* device time of the linear solves */
+    char message[256];
+} nb2_solve_report;
+
+/* One row per Newton iteration: step time, iteration, CG iterations, displacement norm,
+ * residual norm (static_matrix.hpp:385-400). */
+typedef struct nb2_newton_log {
+    double step_time;
+    int32_t iteration;
+    int32_t cg_iterations;
+    double displacement_norm;
+    double force_norm;
+} nb2_newton_log;
+
+/* ---------------------------------------------------------------------------------------- */
+/* Context                                                                                  */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Builds the mesh on the device, the CSR pattern (sparsity_pattern.hpp:18-48: per row the sorted
+ * unique coupled columns, explicit zeros kept), the element->block slot map and the
+ * quadrature-point state (submesh.cpp:26-52).  Replaces solid::mesh / submesh construction. */
+int nb2_create(const nb2_mesh_desc* mesh, const nb2_material* material, nb2_ctx** out);
+int nb2_destroy(nb2_ctx* ctx);
+/* Last error message of this context (or of the last failed nb2_create when ctx is NULL). */
+int nb2_last_error(const nb2_ctx* ctx, char* buffer, size_t size);
+/* Run all work of this context on a caller stream (cudaStream_t passed as void*). */
+int nb2_set_stream(nb2_ctx* ctx, void* stream);
+int nb2_get_sizes(const nb2_ctx* ctx, int32_t* num_dofs, int64_t* nnz, int64_t* num_blocks);
+/* Number of kernels this library launched for the context so far. */
+int nb2_launch_count(const nb2_ctx* ctx, int64_t* launches);
+
+/* Per-element shear modulus (replaces the material G of the microsphere model per element). */
+int nb2_set_element_shear_modulus(nb2_ctx* ctx, const double* shear_modulus);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Element-level drop-ins (host buffers)                                                   */
+/* ---------------------------------------------------------------------------------------- */
+
+/* CSR export, bit-exact with neon's Eigen RowMajor pattern: rowptr[num_dofs+1], col[nnz]
+ * (compute_sparsity_pattern, sparsity_pattern.hpp:18-48). */
+int nb2_export_pattern(nb2_ctx* ctx, int32_t* rowptr, int32_t* col);
+
+/* mesh.update_internal_variables(u, dt) (mesh.cpp:56-70): x = X + u, deformation measures,
+ * det F check, constitutive update of the current (trial) state; stores stress and tangent
+ * coefficients per quadrature point for the calls below. */
+int nb2_update_internal_variables(nb2_ctx* ctx, const double* u, double time_step_size);
+
+/* static_matrix::assemble_stiffness (static_matrix.hpp:243-277) into CSR values K[nnz] and
+ * compute_internal_force (:189-203) into f_int[num_dofs], from the state of the last update.
+ * Either pointer may be NULL. */
+int nb2_assemble(nb2_ctx* ctx, double* K_values, double* f_int);
+
+/* submesh::save_internal_variables (submesh.cpp:54-64): commit (1) or revert (0). */
+int nb2_save_internal_variables(nb2_ctx* ctx, int32_t converged);
+
+/* Quadrature-point outputs of the last update: which = 0 Cauchy stress [nqp][9] (row-major
+ * 3x3), 1 det F [nqp], 2 plastic strain [nqp][9], 3 accumulated plastic strain [nqp]. */
+int nb2_get_quadrature_values(nb2_ctx* ctx, int32_t which, double* out);
+
+/* static_matrix::enforce_dirichlet_conditions (static_matrix.hpp:279-320) on host CSR values
+ * laid out as nb2_export_pattern: zero row and column of each listed DOF, keep the diagonal,
+ * b[dof] = 0. */
+int nb2_apply_dirichlet(nb2_ctx* ctx, const int32_t* dofs, int32_t num_dofs, double* K_values,
+                        double* b);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Linear solver plugin                                                                     */
+/* ---------------------------------------------------------------------------------------- */
+
+/* conjugate_gradient::solve (linear_solver.cpp:67-109) on a caller CSR (host buffers): Jacobi
+ * PCG from x0 = 0, stop when ||r||^2 < max(tol^2 ||b||^2, DBL_MIN); NB2_E_CG_MAXIT when the
+ * iteration count reaches maximum_iterations.  FP64 on the device. */
+int nb2_pcg_solve(int32_t n, const int32_t* rowptr, const int32_t* col, const double* values,
+                  const double* b, double* x, double tolerance, int32_t maximum_iterations,
+                  int32_t* iterations, double* error);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Newton driver: static_matrix                                                             */
+/* ---------------------------------------------------------------------------------------- */
+
+/* static_matrix::solve() (static_matrix.hpp:145-187): adaptive load stepping, full Newton with
+ * Dirichlet lifting, device-resident PCG, commit/revert and cutback.  Dirichlet tables are taken
+ * in the order neon iterates them (boundary names sorted, then x, y, z).  u_out (nullable,
+ * [num_dofs]) receives the final displacement, log (nullable) up to max_log Newton rows. */
+int nb2_static_solve(nb2_ctx* ctx, const nb2_solver_options* options,
+                     const nb2_dof_table* dirichlet, int32_t num_dirichlet,
+                     const nb2_dof_table* nodal_forces, int32_t num_nodal_forces, double* u_out,
+                     nb2_solve_report* report, nb2_newton_log* log, int32_t max_log);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Device-resident stepping (benchmarks and the batched / adjoint harnesses)                */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Upload u (host) into the context's displacement. */
+int nb2_set_displacement(nb2_ctx* ctx, const double* u);
+int nb2_get_displacement(nb2_ctx* ctx, double* u);
+/* One fused device pass at the context's displacement: constitutive update + tangent stiffness
+ * (precision) + internal force, into device-resident K and f_int.  No host copies, no sync. */
+int nb2_update_assemble_device(nb2_ctx* ctx, int32_t precision);
+/* Copy device K (CSR order, FP64 path) / f_int to host. */
+int nb2_download_system(nb2_ctx* ctx, double* K_values, double* f_int);
+int nb2_synchronize(nb2_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEON_B200_H */

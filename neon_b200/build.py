@@ -1,0 +1,66 @@
+"""Build libneon_b200.so in-tree with nvcc for sm_100a.
+
+    python -m neon_b200.build [--verbose-ptxas]
+
+Output: neon_b200/_lib/libneon_b200.so (plus the C++ adapter test driver when requested).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIBDIR, "libneon_b200.so")
+SOURCES = ["api.cu", "elements.cu", "pattern.cu", "pcg.cu", "probe.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose_ptxas: bool = False) -> str:
+    os.makedirs(LIBDIR, exist_ok=True)
+    deps = [os.path.join(CSRC, s) for s in SOURCES] + [
+        os.path.join(CSRC, "nb2_internal.cuh"), os.path.join(CSRC, "host_driver.hpp"),
+        os.path.join(ROOT, "include", "neon_b200.h"),
+        os.path.join(ROOT, "include", "neon_b200_probe.h")]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
+                    "--expt-relaxed-constexpr", "-ccbin", shutil.which("g++") or "g++"]
+    if verbose_ptxas:
+        flags += ["-Xptxas", "-v"]
+    for s in SOURCES:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(objdir, s.replace(".cu", ".o"))
+        if force or _stale(obj, [src] + deps[len(SOURCES):]):
+            cmd = [nvcc()] + flags + ["-c", src, "-o", obj]
+            subprocess.run(cmd, check=True)
+        objs.append(obj)
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-ccbin", shutil.which("g++") or "g++"]
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose_ptxas="--verbose-ptxas" in sys.argv)
+    print(LIB)

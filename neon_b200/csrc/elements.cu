@@ -1,0 +1,668 @@
+// elements.cu -- fused element kernel for sm_100a: deformation measures, constitutive update at
+// every quadrature point, tangent stiffness and internal force, scattered into the block CSR.
+//
+// Reference path (dbeurle/neon):
+//   submesh::update_deformation_measures      src/mesh/mechanics/solid/submesh.cpp:210-237
+//   submesh::update_Jacobian_determinants     submesh.cpp:239-269
+//   constitutive updates                      src/constitutive/mechanics/solid/*.cpp (4 models)
+//   submesh::material_tangent_stiffness       submesh.cpp:136-160   (sum_q B^T D B det J w)
+//   submesh::geometric_tangent_stiffness      submesh.cpp:110-134   (sum_q L^T sigma L det J w, x I3)
+//   submesh::internal_force                   submesh.cpp:82-108
+//   static_matrix::assemble_stiffness         src/assembler/mechanics/static_matrix.hpp:243-277
+//
+// Work decomposition (hex8): a group of 8 lanes owns one element, 4 elements per warp.
+//   phase 0  lane a gathers node a (X, u -> x = u + X) into shared memory;
+//   phase 1  lane l runs quadrature point l in FP64: F0 = X dN, F = x dN, H, F F0^-1, det F check,
+//            the constitutive update (J2 state read/written SoA, coalesced across lanes), the
+//            current-configuration gradient L = dN J^-1 and the per-point tangent coefficients;
+//   phase 2  lane g accumulates its 4-5 of the 36 upper-triangular 3x3 blocks over the 8 points.
+//            All four models have an isotropic tangent in this formulation, plus a rank-one
+//            deviatoric term for plastic J2, so a block is
+//              K_ab = s[lam' La(x)Lb + mu'((La.Lb) I + Lb(x)La) + b (N La)(x)(N Lb)]
+//                     + s (La.sigma.Lb) I   (finite strain)
+//            which equals B_a^T D B_b det J w of the reference for
+//              LE/J2 elastic  D = lam 1(x)1 + 2G I            (isotropic_linear_elasticity.cpp:55-67)
+//              J2 plastic     D = C_e - c1 I_dev + c2 n(x)n   -> lam' = lam + c1/3, mu' = G - c1/2
+//              neo-Hooke      D = lam 1(x)1 + 2(mu - lam ln J) I (compressible_neohooke.cpp:58-88)
+//              microsphere    D = (k+p)1(x)1 - 2p I + P Dbar P with P(tau(x)1)P = 0 and
+//                             P I P = I_dev -> lam' = k + p - 2/9 tr tau, mu' = tr tau/3 - p
+//                             (gaussian_affine_microsphere.cpp:58-74);
+//            the stiffness phase runs in Real (FP64 for parity, FP32 for the mixed path);
+//   phase 3  each lane adds its blocks (and the mirrored lower blocks) with red.global.add into
+//            K[slot], and the force of one node into f_int.
+#include <cmath>
+
+#include "nb2_internal.cuh"
+
+namespace nb2 {
+
+__constant__ double c_dN_hex8[8 * 8 * 3];
+__constant__ double c_w_hex8[8];
+__constant__ double c_dN_tet4[4 * 3];
+__constant__ double c_sphere_r[21 * 3];
+__constant__ double c_sphere_w[21];
+
+// (row, first column, count) of the upper-triangular blocks owned by each lane of a group
+__constant__ int c_seg_hex8[8][6] = {{0, 0, 5, 0, 0, 0}, {0, 5, 3, 7, 7, 1}, {1, 1, 5, 0, 0, 0},
+                                     {1, 6, 2, 6, 6, 2}, {2, 2, 5, 0, 0, 0}, {2, 7, 1, 5, 5, 3},
+                                     {3, 3, 5, 0, 0, 0}, {4, 4, 4, 0, 0, 0}};
+__constant__ int c_seg_tet4[2][6] = {{0, 0, 4, 3, 3, 1}, {1, 1, 3, 2, 2, 2}};
+
+template <int NPE>
+struct Topo;
+template <>
+struct Topo<8> {
+    static constexpr int NQ = 8, G = 8, EPC = 8, MAXB = 5;
+};
+template <>
+struct Topo<4> {
+    static constexpr int NQ = 1, G = 2, EPC = 32, MAXB = 5;
+};
+
+// ---------------------------------------------------------------------------------------
+// 3x3 helpers (row-major).  Determinant: first-row expansion; inverse: cofactors times 1/det
+// with det from the first column -- the fixed-size formulas of the reference's linear algebra.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double det3(const double* m) {
+    return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+           m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+__device__ __forceinline__ void inv3(const double* m, double* r) {
+    double c00 = m[4] * m[8] - m[5] * m[7];
+    double c10 = m[7] * m[2] - m[8] * m[1];
+    double c20 = m[1] * m[5] - m[2] * m[4];
+    double det = c00 * m[0] + c10 * m[3] + c20 * m[6];
+    double id = 1.0 / det;
+    r[0] = c00 * id;
+    r[1] = c10 * id;
+    r[2] = c20 * id;
+    r[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+    r[4] = (m[8] * m[0] - m[6] * m[2]) * id;
+    r[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    r[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+    r[7] = (m[6] * m[1] - m[7] * m[0]) * id;
+    r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+__device__ __forceinline__ void matmul3(const double* a, const double* b, double* c) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            c[i * 3 + j] = a[i * 3 + 0] * b[0 * 3 + j] + a[i * 3 + 1] * b[1 * 3 + j] +
+                           a[i * 3 + 2] * b[2 * 3 + j];
+}
+
+// symmetric tensor as 6 values (11, 22, 33, 23, 13, 12)
+__device__ __forceinline__ double dev_norm6(const double* s) {
+    double tr = (s[0] + s[1] + s[2]) / 3.0;
+    double d0 = s[0] - tr, d1 = s[1] - tr, d2 = s[2] - tr;
+    return sqrt(d0 * d0 + d1 * d1 + d2 * d2 + 2.0 * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5]));
+}
+
+struct QpOut {
+    double sig[6];  // Cauchy stress
+    double lam, mu, b;
+    double N[6];    // J2 flow direction (plastic points)
+};
+
+// ----- constitutive models (FP64) --------------------------------------------------------
+
+// isotropic_linear_elasticity.cpp:27-67
+__device__ __forceinline__ void cm_linear_elastic(const ElementArgs& A, const double* H, QpOut& o) {
+    double e0 = H[0], e1 = H[4], e2 = H[8];
+    double e3 = 0.5 * (H[5] + H[7]), e4 = 0.5 * (H[2] + H[6]), e5 = 0.5 * (H[1] + H[3]);
+    double tr = e0 + e1 + e2;
+    o.sig[0] = A.lambda * tr + 2.0 * A.G * e0;
+    o.sig[1] = A.lambda * tr + 2.0 * A.G * e1;
+    o.sig[2] = A.lambda * tr + 2.0 * A.G * e2;
+    o.sig[3] = 2.0 * A.G * e3;
+    o.sig[4] = 2.0 * A.G * e4;
+    o.sig[5] = 2.0 * A.G * e5;
+    o.lam = A.lambda;
+    o.mu = A.G;
+    o.b = 0.0;
+}
+
+// compressible_neohooke.cpp:17-90
+__device__ __forceinline__ void cm_neo_hooke(const ElementArgs& A, const double* F, double J,
+                                             QpOut& o) {
+    double B[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            B[i * 3 + j] = F[i * 3 + 0] * F[j * 3 + 0] + F[i * 3 + 1] * F[j * 3 + 1] +
+                           F[i * 3 + 2] * F[j * 3 + 2];
+    double lnJ = log(J);
+    double mu = A.G, lam = A.lambda;
+    o.sig[0] = (lam * lnJ + mu * (B[0] - 1.0)) / J;
+    o.sig[1] = (lam * lnJ + mu * (B[4] - 1.0)) / J;
+    o.sig[2] = (lam * lnJ + mu * (B[8] - 1.0)) / J;
+    o.sig[3] = (mu * B[5]) / J;
+    o.sig[4] = (mu * B[2]) / J;
+    o.sig[5] = (mu * B[1]) / J;
+    o.lam = lam;
+    o.mu = mu - lam * lnJ;
+    o.b = 0.0;
+}
+
+// small_strain_J2_plasticity.cpp:30-163; the current plastic state is mutated on every call
+__device__ __forceinline__ bool cm_j2(const ElementArgs& A, long long q, const double* H,
+                                      QpOut& o) {
+    const double G = A.G, lam = A.lambda, Hh = A.H_iso;
+    const long long n = A.nqp;
+    double ep[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) ep[c] = A.ep[c * n + q];
+    double ebar = A.epbar[q];
+    double e0 = H[0] - ep[0], e1 = H[4] - ep[1], e2 = H[8] - ep[2];
+    double e3 = 0.5 * (H[5] + H[7]) - ep[3], e4 = 0.5 * (H[2] + H[6]) - ep[4],
+           e5 = 0.5 * (H[1] + H[3]) - ep[5];
+    double tr = e0 + e1 + e2;
+    double* s = o.sig;
+    s[0] = lam * tr + 2.0 * G * e0;
+    s[1] = lam * tr + 2.0 * G * e1;
+    s[2] = lam * tr + 2.0 * G * e2;
+    s[3] = 2.0 * G * e3;
+    s[4] = 2.0 * G * e4;
+    s[5] = 2.0 * G * e5;
+    const double dn = dev_norm6(s);
+    const double vm = sqrt(3.0 / 2.0) * dn;
+    o.lam = lam;
+    o.mu = G;
+    o.b = 0.0;
+    double f = (vm - 3.0 * G * 0.0) - (A.sigma_y + ebar * Hh);
+    if (f <= 0.0) return true;
+    const double vm_trial = vm;
+    double trs = (s[0] + s[1] + s[2]) / 3.0;
+    double nrm[6] = {(s[0] - trs) / dn, (s[1] - trs) / dn, (s[2] - trs) / dn,
+                     s[3] / dn,         s[4] / dn,         s[5] / dn};
+    double dg = 0.0;
+    int it = 0;
+    while (f > 1.0e-6 && it < 50) {
+        dg += f / (3.0 * G + Hh);
+        f = (vm - 3.0 * G * dg) - (A.sigma_y + (ebar + dg) * Hh);
+        ++it;
+    }
+    if (it == 50) return false;
+    const double s32 = sqrt(3.0 / 2.0);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        A.ep[c * n + q] = ep[c] + dg * s32 * nrm[c];
+        s[c] -= 2.0 * G * dg * s32 * nrm[c];
+    }
+    A.epbar[q] = ebar + dg;
+    double c1 = dg * 6.0 * (G * G) / vm_trial;
+    double c2 = 6.0 * (G * G) * (dg / vm_trial - 1.0 / (3.0 * G + Hh));
+    o.lam = lam + c1 / 3.0;
+    o.mu = G - 0.5 * c1;
+    o.b = c2;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) o.N[c] = nrm[c];
+    return true;
+}
+
+// gaussian_affine_microsphere.cpp:23-88 with volumetric_free_energy.hpp:16-30
+__device__ __forceinline__ void cm_microsphere(const ElementArgs& A, double Gm, const double* F,
+                                               double J, QpOut& o) {
+    const double K = A.K;
+    double sc = pow(det3(F), -1.0 / 3.0);
+    double Fb[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Fb[i] = sc * F[i];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 3
+    for (int i = 0; i < 21; ++i) {
+        double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1], r2 = c_sphere_r[3 * i + 2];
+        double w = c_sphere_w[i];
+        double t0 = Fb[0] * r0 + Fb[1] * r1 + Fb[2] * r2;
+        double t1 = Fb[3] * r0 + Fb[4] * r1 + Fb[5] * r2;
+        double t2 = Fb[6] * r0 + Fb[7] * r1 + Fb[8] * r2;
+        acc[0] += (t0 * t0) * w;
+        acc[1] += (t1 * t1) * w;
+        acc[2] += (t2 * t2) * w;
+        acc[3] += (t1 * t2) * w;
+        acc[4] += (t0 * t2) * w;
+        acc[5] += (t0 * t1) * w;
+    }
+    double tau[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tau[c] = 3.0 * Gm * acc[c];
+    double p = J * (K / 2.0 * (J - 1.0 / J));
+    double trt = tau[0] + tau[1] + tau[2];
+    double tr3 = trt / 3.0;
+    o.sig[0] = (p + tau[0] - tr3) / J;
+    o.sig[1] = (p + tau[1] - tr3) / J;
+    o.sig[2] = (p + tau[2] - tr3) / J;
+    o.sig[3] = tau[3] / J;
+    o.sig[4] = tau[4] / J;
+    o.sig[5] = tau[5] / J;
+    double kappa = (J * J) * (K / 2.0 * (1.0 + 1.0 / (J * J)));
+    o.lam = kappa + p - (2.0 / 9.0) * trt;
+    o.mu = trt / 3.0 - p;
+    o.b = 0.0;
+}
+
+__device__ __forceinline__ void report_status(DeviceStatus* st, int code) {
+    atomicOr(&st->flags, 1u << (code - 1));
+}
+
+// ---------------------------------------------------------------------------------------
+// The kernel
+// ---------------------------------------------------------------------------------------
+template <int NPE, int MODEL, typename Real, int MODE>
+__global__ void __launch_bounds__(64) k_element(ElementArgs A) {
+    using T = Topo<NPE>;
+    constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC, MAXB = T::MAXB;
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
+    constexpr bool kJ2 = (MODEL == MODEL_J2);
+    constexpr bool kCon = (MODE & MODE_CONSTITUTIVE) != 0;
+    constexpr bool kStiff = (MODE & MODE_STIFFNESS) != 0;
+    constexpr bool kForce = (MODE & MODE_FORCE) != 0;
+    constexpr bool kStore = (MODE & MODE_STORE) != 0;
+    constexpr int NV = kJ2 ? NPE * 3 : 1;
+
+    __shared__ double sX[EPC][NPE][3];
+    __shared__ double sx[EPC][NPE][3];
+    __shared__ double sdN[NQ][NPE][3];
+    __shared__ Real sL[EPC][NQ][NPE * 3];
+    __shared__ Real sV[EPC][NQ][NV];
+    __shared__ double sG[EPC][NQ][NPE * 3];
+    __shared__ Real sC[EPC][NQ][4];
+
+    const int tid = threadIdx.x;
+    const int le = tid / G;     // element within the CTA
+    const int lane = tid % G;   // lane within the element group
+    const long long e = (long long)blockIdx.x * EPC + le;
+    const bool valid = e < A.E;
+
+    for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
+        (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
+
+    // phase 0: gather nodes
+    int node[(NPE + G - 1) / G];
+#pragma unroll
+    for (int j = 0; j < (NPE + G - 1) / G; ++j) {
+        int a = lane + j * G;
+        node[j] = 0;
+        if (a < NPE && valid) {
+            int nd = A.conn[e * NPE + a];
+            node[j] = nd;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                double Xv = A.X[3ll * nd + k];
+                sX[le][a][k] = Xv;
+                sx[le][a][k] = A.u[3ll * nd + k] + Xv;
+            }
+        }
+    }
+    __syncthreads();
+
+    // phase 1: quadrature points
+    for (int l = lane; l < NQ; l += G) {
+        if (!valid) break;
+        const double w = (NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0);
+        const long long q = e * NQ + l;
+        double Fc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) Fc[i * 3 + k] += sx[le][a][i] * sdN[l][a][k];
+        QpOut o;
+        if constexpr (kCon) {
+            double F0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) F0[i * 3 + k] += sX[le][a][i] * sdN[l][a][k];
+            double F0i[9];
+            inv3(F0, F0i);
+            double Hm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                double b0[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    b0[k] = sdN[l][a][0] * F0i[0 * 3 + k] + sdN[l][a][1] * F0i[1 * 3 + k] +
+                            sdN[l][a][2] * F0i[2 * 3 + k];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    double d = sx[le][a][i] - sX[le][a][i];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) Hm[i * 3 + k] += d * b0[k];
+                }
+            }
+            double Fd[9];
+            matmul3(Fc, F0i, Fd);
+            const double detF = det3(Fd);
+            if (signbit(detF)) {
+                unsigned long long key = ((unsigned long long)q << 32) |
+                                         (unsigned long long)__float_as_uint((float)detF);
+                atomicMin(&A.status->negdet_first, key);
+                atomicAdd(&A.status->negdet_count, 1u);
+                report_status(A.status, NB2_E_NEG_DETJ);
+            }
+            if constexpr (MODEL == MODEL_LE) {
+                cm_linear_elastic(A, Hm, o);
+            } else if constexpr (MODEL == MODEL_NH) {
+                cm_neo_hooke(A, Fd, detF, o);
+            } else if constexpr (MODEL == MODEL_J2) {
+                if (!cm_j2(A, q, Hm, o)) report_status(A.status, NB2_E_RETURN_MAP);
+            } else {
+                cm_microsphere(A, A.Ge ? A.Ge[e] : A.G, Fd, detF, o);
+            }
+            bool bad = isnan(o.lam) || isnan(o.mu);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) bad |= isnan(o.sig[c]);
+            if (bad) report_status(A.status, NB2_E_NAN);
+            if constexpr (kStore) {
+                const long long n = A.nqp;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) A.sig[c * n + q] = o.sig[c];
+                A.dpar[0 * n + q] = o.lam;
+                A.dpar[1 * n + q] = o.mu;
+                A.dpar[2 * n + q] = o.b;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) A.dpar[(3 + c) * n + q] = kJ2 ? o.N[c] : 0.0;
+                A.detF[q] = detF;
+            }
+        } else {
+            const long long n = A.nqp;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) o.sig[c] = A.sig[c * n + q];
+            o.lam = A.dpar[0 * n + q];
+            o.mu = A.dpar[1 * n + q];
+            o.b = A.dpar[2 * n + q];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) o.N[c] = A.dpar[(3 + c) * n + q];
+        }
+        if constexpr (kStiff || kForce) {
+            double Ji[9];
+            inv3(Fc, Ji);
+            const double s = w * det3(Fc);
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                double La[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    La[k] = sdN[l][a][0] * Ji[0 * 3 + k] + sdN[l][a][1] * Ji[1 * 3 + k] +
+                            sdN[l][a][2] * Ji[2 * 3 + k];
+                // g_a = s sigma L_a  (sigma symmetric: 11 22 33 23 13 12)
+                sG[le][l][3 * a + 0] = s * (o.sig[0] * La[0] + o.sig[5] * La[1] + o.sig[4] * La[2]);
+                sG[le][l][3 * a + 1] = s * (o.sig[5] * La[0] + o.sig[1] * La[1] + o.sig[3] * La[2]);
+                sG[le][l][3 * a + 2] = s * (o.sig[4] * La[0] + o.sig[3] * La[1] + o.sig[2] * La[2]);
+                if constexpr (kStiff) {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) sL[le][l][3 * a + k] = (Real)La[k];
+                    if constexpr (kJ2) {
+                        sV[le][l][3 * a + 0] = (Real)(o.N[0] * La[0] + o.N[5] * La[1] + o.N[4] * La[2]);
+                        sV[le][l][3 * a + 1] = (Real)(o.N[5] * La[0] + o.N[1] * La[1] + o.N[3] * La[2]);
+                        sV[le][l][3 * a + 2] = (Real)(o.N[4] * La[0] + o.N[3] * La[1] + o.N[2] * La[2]);
+                    }
+                }
+            }
+            sC[le][l][0] = (Real)(s * o.lam);
+            sC[le][l][1] = (Real)(s * o.mu);
+            sC[le][l][2] = (Real)(s * o.b);
+            sC[le][l][3] = (Real)0;
+        }
+    }
+    __syncthreads();
+    if (!valid) return;
+
+    if constexpr (kForce) {
+        // internal force of node a: sum_q g_a(q)
+#pragma unroll
+        for (int j = 0; j < (NPE + G - 1) / G; ++j) {
+            int a = lane + j * G;
+            if (a < NPE) {
+                double f0 = 0, f1 = 0, f2 = 0;
+#pragma unroll
+                for (int l = 0; l < NQ; ++l) {
+                    f0 += sG[le][l][3 * a + 0];
+                    f1 += sG[le][l][3 * a + 1];
+                    f2 += sG[le][l][3 * a + 2];
+                }
+                atomicAdd(&A.fint[3ll * node[j] + 0], f0);
+                atomicAdd(&A.fint[3ll * node[j] + 1], f1);
+                atomicAdd(&A.fint[3ll * node[j] + 2], f2);
+            }
+        }
+    }
+
+    if constexpr (kStiff) {
+        const int* seg = (NPE == 8) ? c_seg_hex8[lane] : c_seg_tet4[lane];
+        const int r0 = seg[0], b0s = seg[1], n0 = seg[2], r1 = seg[3], b1s = seg[4], n1 = seg[5];
+        Real acc[MAXB][9];
+#pragma unroll
+        for (int j = 0; j < MAXB; ++j)
+#pragma unroll
+            for (int i = 0; i < 9; ++i) acc[j][i] = (Real)0;
+
+        for (int l = 0; l < NQ; ++l) {
+            const Real cl = sC[le][l][0], cm = sC[le][l][1], cb = sC[le][l][2];
+            Real L0[3], L1[3], g0[3], g1[3], v0[3], v1[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                L0[k] = sL[le][l][3 * r0 + k];
+                L1[k] = sL[le][l][3 * r1 + k];
+                if constexpr (kFinite) {
+                    g0[k] = (Real)sG[le][l][3 * r0 + k];
+                    g1[k] = (Real)sG[le][l][3 * r1 + k];
+                }
+                if constexpr (kJ2) {
+                    v0[k] = sV[le][l][3 * r0 + k];
+                    v1[k] = sV[le][l][3 * r1 + k];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < MAXB; ++j) {
+                const bool in0 = j < n0;
+                if (j < n0 + n1) {
+                    const int b = in0 ? b0s + j : b1s + (j - n0);
+                    Real La[3], Lb[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        La[k] = in0 ? L0[k] : L1[k];
+                        Lb[k] = sL[le][l][3 * b + k];
+                    }
+                    Real d = La[0] * Lb[0] + La[1] * Lb[1] + La[2] * Lb[2];
+                    Real diag = cm * d;
+                    if constexpr (kFinite) {
+                        diag += (in0 ? g0[0] : g1[0]) * Lb[0] + (in0 ? g0[1] : g1[1]) * Lb[1] +
+                                (in0 ? g0[2] : g1[2]) * Lb[2];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            Real v = cl * La[i] * Lb[k] + cm * La[k] * Lb[i];
+                            if (i == k) v += diag;
+                            acc[j][3 * i + k] += v;
+                        }
+                    if constexpr (kJ2) {
+                        if (cb != (Real)0) {
+                            Real va[3], vb[3];
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                va[k] = in0 ? v0[k] : v1[k];
+                                vb[k] = sV[le][l][3 * b + k];
+                            }
+#pragma unroll
+                            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                                for (int k = 0; k < 3; ++k) acc[j][3 * i + k] += cb * va[i] * vb[k];
+                        }
+                    }
+                }
+            }
+        }
+
+        // phase 3: scatter (red.global.add) of the upper blocks and their transposes
+        const int* slot = A.slot + e * (NPE * NPE);
+#pragma unroll
+        for (int j = 0; j < MAXB; ++j) {
+            if (j < n0 + n1) {
+                const bool in0 = j < n0;
+                const int a = in0 ? r0 : r1;
+                const int b = in0 ? b0s + j : b1s + (j - n0);
+                const long long sab = slot[a * NPE + b];
+                Real* Kp = nullptr;
+                if constexpr (sizeof(Real) == 8)
+                    Kp = reinterpret_cast<Real*>(A.K64);
+                else
+                    Kp = reinterpret_cast<Real*>(A.K32);
+#pragma unroll
+                for (int i = 0; i < 9; ++i) atomicAdd(&Kp[9 * sab + i], acc[j][i]);
+                if (a != b) {
+                    const long long sba = slot[b * NPE + a];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            atomicAdd(&Kp[9 * sba + 3 * k + i], acc[j][3 * i + k]);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+static bool g_tables_ready = false;
+
+static int upload_tables(nb2_ctx* c) {
+    if (g_tables_ready) return NB2_OK;
+    // hexahedron8 shape derivatives at the 8-point rule (hexahedron.cpp:10-67,
+    // hexahedron_quadrature.cpp:27-40)
+    const double lc[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                             {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+    const double g = 1.0 / std::sqrt(3.0);
+    const double qc[8][3] = {{-g, -g, -g}, {g, -g, -g}, {g, g, -g}, {-g, g, -g},
+                             {-g, -g, g},  {g, -g, g},  {g, g, g},  {-g, g, g}};
+    double dN[8 * 8 * 3], w[8];
+    for (int l = 0; l < 8; ++l) {
+        w[l] = 1.0;
+        for (int a = 0; a < 8; ++a) {
+            double xa = lc[a][0], ea = lc[a][1], za = lc[a][2];
+            double xi = qc[l][0], eta = qc[l][1], zeta = qc[l][2];
+            dN[(l * 8 + a) * 3 + 0] = 1.0 / 8.0 * xa * (1.0 + ea * eta) * (1.0 + za * zeta);
+            dN[(l * 8 + a) * 3 + 1] = 1.0 / 8.0 * (1.0 + xa * xi) * ea * (1.0 + za * zeta);
+            dN[(l * 8 + a) * 3 + 2] = 1.0 / 8.0 * (1.0 + xa * xi) * (1.0 + ea * eta) * za;
+        }
+    }
+    // tetrahedron4 (tetrahedron.cpp:6-45)
+    const double dNt[12] = {1, 0, 0, 0, 1, 0, 0, 0, 1, -1, -1, -1};
+    // BO21 (unit_sphere_quadrature.cpp:10-31)
+    const double w1 = 0.0265214244093 * 2.0, w2 = 0.0199301476312 * 2.0, w3 = 0.0250712367487 * 2.0;
+    const double d0 = 0.707106781187, d1 = 0.387907304067, d2 = 0.836095596749;
+    const double r[21 * 3] = {1, 0, 0, 0, 1, 0, 0, 0, 1, d0, d0, 0, d0, -d0, 0, d0, 0, d0, d0, 0, -d0,
+                              0, d0, d0, 0, d0, -d0, d1, d1, d2, d1, d1, -d2, d1, -d1, d2, d1, -d1,
+                              -d2, d1, d2, d1, d1, d2, -d1, d1, -d2, d1, d1, -d2, -d1, d2, d1, d1,
+                              d2, d1, -d1, d2, -d1, d1, d2, -d1, -d1};
+    double sw[21];
+    for (int i = 0; i < 21; ++i) sw[i] = i < 3 ? w1 : (i < 9 ? w2 : w3);
+    NB2_CUDA(c, cudaMemcpyToSymbol(c_dN_hex8, dN, sizeof dN));
+    NB2_CUDA(c, cudaMemcpyToSymbol(c_w_hex8, w, sizeof w));
+    NB2_CUDA(c, cudaMemcpyToSymbol(c_dN_tet4, dNt, sizeof dNt));
+    NB2_CUDA(c, cudaMemcpyToSymbol(c_sphere_r, r, sizeof r));
+    NB2_CUDA(c, cudaMemcpyToSymbol(c_sphere_w, sw, sizeof sw));
+    g_tables_ready = true;
+    return NB2_OK;
+}
+
+template <int NPE, int MODEL, typename Real, int MODE>
+static void launch_one(nb2_ctx* c, const ElementArgs& A) {
+    constexpr int EPC = Topo<NPE>::EPC, G = Topo<NPE>::G;
+    unsigned grid = (unsigned)((c->E + EPC - 1) / EPC);
+    k_element<NPE, MODEL, Real, MODE><<<grid, EPC * G, 0, c->stream>>>(A);
+    c->launches++;
+}
+
+template <int NPE, int MODEL>
+static int dispatch_mode(nb2_ctx* c, const ElementArgs& A, int mode, int precision) {
+    constexpr int FUSED = MODE_CONSTITUTIVE | MODE_STIFFNESS | MODE_FORCE;
+    constexpr int RESID = MODE_CONSTITUTIVE | MODE_FORCE;
+    constexpr int UPD = MODE_CONSTITUTIVE | MODE_STORE;
+    constexpr int ASM = MODE_STIFFNESS | MODE_FORCE;
+    if (mode == FUSED && precision == NB2_FP64) launch_one<NPE, MODEL, double, FUSED>(c, A);
+    else if (mode == FUSED) launch_one<NPE, MODEL, float, FUSED>(c, A);
+    else if (mode == RESID) launch_one<NPE, MODEL, double, RESID>(c, A);
+    else if (mode == UPD) launch_one<NPE, MODEL, double, UPD>(c, A);
+    else if (mode == ASM) launch_one<NPE, MODEL, double, ASM>(c, A);
+    else return NB2_E_INPUT;
+    return NB2_OK;
+}
+
+template <int NPE>
+static int dispatch_model(nb2_ctx* c, const ElementArgs& A, int mode, int precision) {
+    switch (c->mat.model) {
+        case MODEL_LE: return dispatch_mode<NPE, MODEL_LE>(c, A, mode, precision);
+        case MODEL_NH: return dispatch_mode<NPE, MODEL_NH>(c, A, mode, precision);
+        case MODEL_J2: return dispatch_mode<NPE, MODEL_J2>(c, A, mode, precision);
+        case MODEL_MS: return dispatch_mode<NPE, MODEL_MS>(c, A, mode, precision);
+    }
+    return NB2_E_INPUT;
+}
+
+int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
+    int st = upload_tables(c);
+    if (st) return st;
+    ElementArgs A;
+    A.X = c->X;
+    A.u = c->u;
+    A.conn = c->conn;
+    A.slot = c->slot;
+    A.E = c->E;
+    A.nqp = c->nqp;
+    A.K = c->mat.bulk_modulus;
+    A.G = c->mat.shear_modulus;
+    A.lambda = c->mat.bulk_modulus - 2.0 * c->mat.shear_modulus / 3.0;
+    A.sigma_y = c->mat.yield_stress;
+    A.H_iso = c->mat.isotropic_hardening_modulus;
+    A.Ge = c->Ge;
+    A.ep = c->ep;
+    A.epbar = c->epbar;
+    A.K64 = c->K64;
+    A.K32 = c->K32;
+    A.fint = c->fint;
+    A.sig = c->sig;
+    A.dpar = c->dpar;
+    A.detF = c->detF;
+    A.status = c->status;
+    if (mode & MODE_STIFFNESS) {
+        if (precision == NB2_FP64)
+            NB2_CUDA(c, cudaMemsetAsync(c->K64, 0, sizeof(double) * 9 * c->nnzb, c->stream));
+        else
+            NB2_CUDA(c, cudaMemsetAsync(c->K32, 0, sizeof(float) * 9 * c->nnzb, c->stream));
+    }
+    if (mode & MODE_FORCE) NB2_CUDA(c, cudaMemsetAsync(c->fint, 0, sizeof(double) * c->n, c->stream));
+    st = (c->npe == 8) ? dispatch_model<8>(c, A, mode, precision)
+                       : dispatch_model<4>(c, A, mode, precision);
+    if (st) return st;
+    NB2_CUDA(c, cudaGetLastError());
+    return NB2_OK;
+}
+
+// Canonical algorithmic FLOPs per element (hex8 small strain 29,040; hex8 finite strain 32,240;
+// tet4 finite strain 1,552) plus the constitutive update per point (LE 60, NH 120, J2 250,
+// microsphere BO21 2,000).
+void element_flop_model(const nb2_ctx* c, double* flops_per_element) {
+    double base;
+    bool finite = c->mat.model == MODEL_NH || c->mat.model == MODEL_MS;
+    if (c->npe == 8)
+        base = finite ? 32240.0 : 29040.0;
+    else
+        base = 1552.0;
+    const double cm[4] = {60.0, 120.0, 250.0, 2000.0};
+    *flops_per_element = base + c->nq * cm[c->mat.model];
+}
+
+}  // namespace nb2

@@ -1,0 +1,173 @@
+// nb2_internal.cuh -- context layout and device helpers shared by the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/neon_b200.h"
+
+namespace nb2 {
+
+// ---------------------------------------------------------------------------------------
+// Device layout
+//
+//   nodes        X[N][3], u[N][3]  (node-major: DOF 3*node + k, gathers read 24 B per node)
+//   elements     conn[E][npe]      (element-major: a group of lanes reads one element's row)
+//   block pattern brp[N+1], bcol[nnzb]  (3x3 node blocks; CSR of neon = this pattern expanded)
+//   values       K[nnzb][9]        (row-major 3x3 block, FP64 or FP32)
+//   slot map     slot[E][npe*npe]  (block index of element block (a,b))
+//   qp state     SoA: ep[6][nqp], epbar[nqp] (current) and their committed copies
+//   qp outputs   sig[6][nqp], dpar[9][nqp], detF[nqp] (only for the split update/assemble path)
+// ---------------------------------------------------------------------------------------
+
+enum : int { MODEL_LE = 0, MODEL_NH = 1, MODEL_J2 = 2, MODEL_MS = 3 };
+
+// element-kernel mode bits
+enum : int {
+    MODE_CONSTITUTIVE = 1,  // compute the constitutive update from u (else load stored outputs)
+    MODE_STIFFNESS = 2,     // accumulate + scatter the tangent stiffness
+    MODE_FORCE = 4,         // accumulate + scatter the internal force
+    MODE_STORE = 8,         // store stress / tangent coefficients / det F per quadrature point
+};
+
+struct DeviceStatus {
+    unsigned int flags;                // bit (status code - 1)
+    unsigned int negdet_count;
+    unsigned long long negdet_first;   // (qp index << 32) | float bits of det F
+};
+
+struct ElementArgs {
+    const double* X;
+    const double* u;
+    const int* conn;
+    const int* slot;
+    int E;
+    int nqp;
+    double K, G, lambda, sigma_y, H_iso;
+    const double* Ge;
+    double* ep;      // [6][nqp]
+    double* epbar;   // [nqp]
+    double* K64;     // [nnzb][9]
+    float* K32;
+    double* fint;    // [3N]
+    double* sig;     // [6][nqp]
+    double* dpar;    // [9][nqp]
+    double* detF;    // [nqp]
+    DeviceStatus* status;
+};
+
+// PCG scalars kept on the device (no host round trip per iteration)
+struct CgScalars {
+    double rhs_norm2, threshold;
+    double abs_new, pq, alpha, rr, rz, beta;
+    int iterations, max_iterations, done, status;
+    unsigned int counter[4];  // last-block tickets of the reductions
+};
+
+struct Timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+
+}  // namespace nb2
+
+struct nb2_ctx {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int N = 0, E = 0, npe = 0, nq = 0, nqp = 0, n = 0;
+    long long nnzb = 0, nnz = 0;
+    nb2_material mat{};
+
+    // mesh + pattern
+    double* X = nullptr;
+    int* conn = nullptr;
+    int* brp = nullptr;
+    int* bcol = nullptr;
+    int* slot = nullptr;
+    std::vector<int> h_brp, h_bcol;  // host copy of the block pattern
+
+    // values and vectors
+    double* K64 = nullptr;
+    float* K32 = nullptr;
+    double* u = nullptr;
+    double* u_old = nullptr;
+    double* fint = nullptr;
+    double* fext = nullptr;
+    double* rhs = nullptr;  // minus_residual
+    double* du = nullptr;   // delta_d
+    double* inc = nullptr;  // prescribed increment
+    unsigned char* mask = nullptr;  // active Dirichlet DOFs
+    double* Ge = nullptr;
+
+    // quadrature-point state
+    double* ep = nullptr;
+    double* epbar = nullptr;
+    double* ep_old = nullptr;
+    double* epbar_old = nullptr;
+    double* sig = nullptr;
+    double* dpar = nullptr;
+    double* detF = nullptr;
+
+    // PCG workspace (FP64 and FP32 views share nothing)
+    double *cg_x = nullptr, *cg_r = nullptr, *cg_p = nullptr, *cg_q = nullptr, *cg_inv = nullptr;
+    float *cg32_x = nullptr, *cg32_r = nullptr, *cg32_p = nullptr, *cg32_q = nullptr,
+          *cg32_inv = nullptr;
+    double* partials = nullptr;  // reduction partials
+    nb2::CgScalars* cgs = nullptr;
+    nb2::CgScalars* h_cgs = nullptr;  // pinned mirror
+    double* norms = nullptr;          // device norm results
+    double* h_norms = nullptr;        // pinned mirror
+    nb2::DeviceStatus* status = nullptr;
+
+    cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;  // captured CG iteration blocks
+
+    long long launches = 0;
+    std::string error;
+};
+
+namespace nb2 {
+
+// launch geometry of the reduction kernels: persistent grid, fixed partial count
+constexpr int kRedThreads = 256;
+int reduction_blocks(const nb2_ctx* c);
+
+// CUDA error -> context message + status
+int cuda_fail(nb2_ctx* c, cudaError_t e, const char* what);
+#define NB2_CUDA(ctx, call)                                     \
+    do {                                                        \
+        cudaError_t _e = (call);                                \
+        if (_e != cudaSuccess) return nb2::cuda_fail(ctx, _e, #call); \
+    } while (0)
+
+// pattern.cu
+int build_pattern(nb2_ctx* c);
+int export_csr_values(nb2_ctx* c, const double* Kbsr, double* Kcsr_dev);
+
+// elements.cu
+int launch_element_kernel(nb2_ctx* c, int mode, int precision);
+void element_flop_model(const nb2_ctx* c, double* flops_per_element);
+
+// pcg.cu
+struct BsrView {
+    const int* brp;
+    const int* bcol;
+    int nrows_block;  // N
+};
+int pcg_device_fp64(nb2_ctx* c, const double* b, double* x, double tol, int maxit, bool use_mask,
+                    int* iterations, double* error, bool use_graphs);
+int pcg_device_fp32(nb2_ctx* c, const double* b, double* x, double tol, int maxit, int* iterations,
+                    double* error, bool use_graphs);
+int pcg_csr_host(int n, const int* rowptr, const int* col, const double* val, const double* b,
+                 double* x, double tol, int maxit, int* iterations, double* error,
+                 std::string* err);
+void release_graphs(nb2_ctx* c);
+void bsr_spmv_fp64(nb2_ctx* c, const double* x, double* y, bool use_mask);
+void bsr_spmv_mixed_accum(nb2_ctx* c, const double* x, double* y);  // y = K32 x in FP64 accum
+// five norms ||du||, ||u||, ||rhs||, ||fext||, ||fint|| into c->h_norms (synchronises)
+int compute_norms(nb2_ctx* c);
+double device_dot_sync(nb2_ctx* c, const double* a, const double* b, int n);
+
+}  // namespace nb2

@@ -1,0 +1,601 @@
+// pcg.cu -- Jacobi-preconditioned CG on the device for sm_100a.
+//
+// Reference: conjugate_gradient::solve (src/solver/linear/linear_solver.cpp:67-109), which runs
+// Eigen's ConjugateGradient<Lower|Upper> with the diagonal preconditioner, x0 = 0 and the stop
+// test ||r||^2 < max(tol^2 ||b||^2, DBL_MIN), and the reference's GPU variant
+// conjugate_gradient_cuda::solve (conjugate_gradient_cuda.cpp:72-192, cuSPARSE csrmv + cuBLAS
+// + diagonal_matrix_vector_product.cu) which copies K to the device on every solve and reads 3
+// dot products back to the host per iteration.
+//
+// Here K stays resident in HBM and every scalar stays on the device.  One iteration is three
+// kernels:
+//   k_spmv  : q = A p over the 3x3 block rows (one warp per block row, values streamed with
+//             evict-first loads so p stays in L2), fused with the p.q reduction; the last block
+//             to finish forms alpha = (r.z)/(p.q);
+//   k_xr    : x += alpha p, r -= alpha q, fused with r.r and r.z (z = D^-1 r); the last block
+//             applies the stop test, beta and the iteration count;
+//   k_p     : p = D^-1 r + beta p.
+// Reductions are per-block partials summed in a fixed order by the last block (deterministic,
+// no spin waits).  Kernels return at once after `done` is set, so whole blocks of iterations are
+// enqueued (optionally as one CUDA graph) and the host reads the flag once per block.
+// Rows of active Dirichlet DOFs are skipped (q = 0): with b = 0 there, r, z, p stay exactly 0 on
+// them, so this equals neon's zeroing of those rows and columns (static_matrix.hpp:279-320).
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "nb2_internal.cuh"
+
+namespace nb2 {
+
+int reduction_blocks(const nb2_ctx*) { return 148 * 4; }
+
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T* p) {
+    return __ldcs(p);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of NV doubles into partials[blockIdx*NV + j]; returns true in the last block
+// (after which s_red holds nothing useful and the caller reduces partials itself).
+template <int NV>
+__device__ bool block_partials(double (&v)[NV], double* partials, unsigned int* counter) {
+    __shared__ double red[NV][kRedThreads / 32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double t = warp_sum(v[j]);
+        if (lane == 0) red[j][wid] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            double t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[j][w];
+            partials[blockIdx.x * NV + j] = t;
+        }
+        __threadfence();
+        unsigned int ticket = atomicAdd(counter, 1u);
+        last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    return last;
+}
+
+// Fixed-order sum of partials[b*NV + j] over b (called by the whole last block).
+template <int NV>
+__device__ void final_sum(const double* partials, double (&out)[NV]) {
+    __shared__ double red[NV][kRedThreads];
+    __threadfence();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double t = 0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+            t += *((volatile const double*)&partials[b * NV + j]);
+        red[j][threadIdx.x] = t;
+    }
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+#pragma unroll
+            for (int j = 0; j < NV; ++j) red[j][threadIdx.x] += red[j][threadIdx.x + s];
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < NV; ++j) out[j] = red[j][0];
+}
+
+// ---------------------------------------------------------------------------------------
+// matrices
+// ---------------------------------------------------------------------------------------
+template <typename V>
+struct Bsr {
+    const int* brp;
+    const int* bcol;
+    const V* val;
+    int rows;  // block rows
+};
+
+struct Csr {
+    const int* rp;
+    const int* ci;
+    const double* val;
+    int rows;
+};
+
+// y[3a+r] for r = 0..2 of block row a, reduced across the warp; returned in lane 0.
+template <typename V, typename X, typename Acc>
+__device__ __forceinline__ void bsr_row(const Bsr<V>& A, const X* __restrict__ x, int a, int lane,
+                                        Acc& y0, Acc& y1, Acc& y2) {
+    const int b0 = A.brp[a];
+    const int deg = A.brp[a + 1] - b0;
+    const V* vals = A.val + 9ll * b0;
+    const int* cols = A.bcol + b0;
+    Acc a0 = 0, a1 = 0, a2 = 0;
+    for (int v = lane; v < 9 * deg; v += 32) {
+        const int k = v / 9;
+        const int e = v - 9 * k;
+        const int r = e / 3;
+        const int cc = e - 3 * r;
+        const Acc prod = (Acc)ld_stream(vals + v) * (Acc)x[3ll * __ldg(cols + k) + cc];
+        a0 += (r == 0) ? prod : (Acc)0;
+        a1 += (r == 1) ? prod : (Acc)0;
+        a2 += (r == 2) ? prod : (Acc)0;
+    }
+    y0 = warp_sum(a0);
+    y1 = warp_sum(a1);
+    y2 = warp_sum(a2);
+}
+
+// ---------------------------------------------------------------------------------------
+// CG kernels (BSR)
+// ---------------------------------------------------------------------------------------
+template <typename V, typename X>
+__global__ void __launch_bounds__(kRedThreads) k_spmv(Bsr<V> A, const X* __restrict__ p,
+                                                      X* __restrict__ q,
+                                                      const unsigned char* __restrict__ mask,
+                                                      CgScalars* s, double* partials) {
+    if (s->done) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    double dot[1] = {0.0};
+    for (int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); a < A.rows; a += warps) {
+        X y0, y1, y2;
+        bsr_row<V, X, X>(A, p, a, lane, y0, y1, y2);
+        if (lane < 3) {
+            const long long i = 3ll * a + lane;
+            X y = lane == 0 ? y0 : (lane == 1 ? y1 : y2);
+            if (mask && mask[i]) y = (X)0;
+            q[i] = y;
+            dot[0] += (double)p[i] * (double)y;
+        }
+    }
+    if (block_partials<1>(dot, partials, &s->counter[0])) {
+        double tot[1];
+        final_sum<1>(partials, tot);
+        if (threadIdx.x == 0) {
+            s->pq = tot[0];
+            s->alpha = s->abs_new / tot[0];
+            if (!(tot[0] > 0.0) || !isfinite(s->alpha)) {
+                s->status = NB2_E_CG_BREAKDOWN;
+                s->done = 1;
+            }
+            s->counter[0] = 0;
+        }
+    }
+}
+
+template <typename X>
+__global__ void __launch_bounds__(kRedThreads) k_xr(long long n, X* __restrict__ x,
+                                                    X* __restrict__ r, const X* __restrict__ p,
+                                                    const X* __restrict__ q,
+                                                    const X* __restrict__ inv, CgScalars* s,
+                                                    double* partials) {
+    if (s->done) return;
+    const X alpha = (X)s->alpha;
+    double acc[2] = {0.0, 0.0};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        X ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        acc[0] += (double)ri * (double)ri;
+        acc[1] += (double)ri * (double)(inv[i] * ri);
+    }
+    if (block_partials<2>(acc, partials, &s->counter[1])) {
+        double tot[2];
+        final_sum<2>(partials, tot);
+        if (threadIdx.x == 0) {
+            s->rr = tot[0];
+            if (tot[0] < s->threshold) {
+                s->done = 1;
+            } else {
+                s->beta = tot[1] / s->abs_new;
+                s->abs_new = tot[1];
+                s->rz = tot[1];
+                s->iterations += 1;
+                if (s->iterations >= s->max_iterations) {
+                    s->done = 1;
+                    s->status = NB2_E_CG_MAXIT;
+                }
+            }
+            if (!isfinite(tot[0])) {
+                s->done = 1;
+                s->status = NB2_E_NAN;
+            }
+            s->counter[1] = 0;
+        }
+    }
+}
+
+template <typename X>
+__global__ void __launch_bounds__(kRedThreads) k_p(long long n, X* __restrict__ p,
+                                                   const X* __restrict__ r,
+                                                   const X* __restrict__ inv, const CgScalars* s) {
+    if (s->done) return;
+    const X beta = (X)s->beta;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        p[i] = inv[i] * r[i] + beta * p[i];
+}
+
+// x = 0, r = b (as X), p = D^-1 r; rhs_norm2, r.r, r.p; threshold and early exits.
+template <typename X>
+__global__ void __launch_bounds__(kRedThreads) k_init(long long n, const double* __restrict__ b,
+                                                      X* __restrict__ x, X* __restrict__ r,
+                                                      X* __restrict__ p,
+                                                      const X* __restrict__ inv, CgScalars* s,
+                                                      double* partials, double tol) {
+    double acc[3] = {0, 0, 0};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        X bi = (X)b[i];
+        x[i] = (X)0;
+        r[i] = bi;
+        X pi = inv[i] * bi;
+        p[i] = pi;
+        acc[0] += b[i] * b[i];
+        acc[1] += (double)bi * (double)bi;
+        acc[2] += (double)bi * (double)pi;
+    }
+    if (block_partials<3>(acc, partials, &s->counter[2])) {
+        double tot[3];
+        final_sum<3>(partials, tot);
+        if (threadIdx.x == 0) {
+            s->rhs_norm2 = tot[0];
+            s->threshold = fmax(tol * tol * tot[0], DBL_MIN);
+            s->rr = tot[1];
+            s->abs_new = tot[2];
+            s->rz = tot[2];
+            s->iterations = 0;
+            s->status = 0;
+            s->done = 0;
+            if (tot[0] == 0.0) {
+                s->done = 1;
+                s->rr = 0.0;
+            } else if (tot[1] < s->threshold) {
+                s->done = 1;
+            }
+            s->counter[2] = 0;
+        }
+    }
+}
+
+// Jacobi inverse diagonal of a block matrix: 1/K_ii, or 1 for a zero diagonal (Eigen's
+// DiagonalPreconditioner).
+template <typename V, typename X>
+__global__ void k_invdiag(Bsr<V> A, X* __restrict__ inv) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= A.rows) return;
+    int lo = A.brp[a], hi = A.brp[a + 1] - 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (A.bcol[mid] < a)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        V d = A.val[9ll * lo + 4 * r];
+        inv[3ll * a + r] = (d != (V)0) ? (X)(1.0 / (double)d) : (X)1;
+    }
+}
+
+template <typename X>
+__global__ void k_copy_out(long long n, const X* __restrict__ src, double* __restrict__ dst) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
+
+// ---------------------------------------------------------------------------------------
+// generic CSR (drop-in linear_solver on a caller matrix)
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRedThreads) k_csr_spmv(Csr A, const double* __restrict__ p,
+                                                          double* __restrict__ q, CgScalars* s,
+                                                          double* partials) {
+    if (s->done) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    double dot[1] = {0.0};
+    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < A.rows; i += warps) {
+        double acc = 0;
+        for (int k = A.rp[i] + lane; k < A.rp[i + 1]; k += 32) acc += A.val[k] * p[A.ci[k]];
+        acc = warp_sum(acc);
+        if (lane == 0) {
+            q[i] = acc;
+            dot[0] += p[i] * acc;
+        }
+    }
+    if (block_partials<1>(dot, partials, &s->counter[0])) {
+        double tot[1];
+        final_sum<1>(partials, tot);
+        if (threadIdx.x == 0) {
+            s->pq = tot[0];
+            s->alpha = s->abs_new / tot[0];
+            if (!isfinite(s->alpha)) {
+                s->status = NB2_E_NAN;
+                s->done = 1;
+            }
+            s->counter[0] = 0;
+        }
+    }
+}
+
+__global__ void k_csr_invdiag(Csr A, double* inv) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.rows) return;
+    double v = 1.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        if (A.ci[k] == i) {
+            if (A.val[k] != 0.0) v = 1.0 / A.val[k];
+            break;
+        }
+    inv[i] = v;
+}
+
+// ---------------------------------------------------------------------------------------
+// norms and helpers
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRedThreads) k_norms(long long n, const double* a,
+                                                       const double* b, const double* c,
+                                                       const double* d, const double* e,
+                                                       double* partials, unsigned int* counter,
+                                                       double* out) {
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        acc[0] += a[i] * a[i];
+        acc[1] += b[i] * b[i];
+        acc[2] += c[i] * c[i];
+        acc[3] += d[i] * d[i];
+        acc[4] += e[i] * e[i];
+    }
+    if (block_partials<5>(acc, partials, counter)) {
+        double tot[5];
+        final_sum<5>(partials, tot);
+        if (threadIdx.x == 0) {
+            for (int j = 0; j < 5; ++j) out[j] = sqrt(tot[j]);
+            *counter = 0;
+        }
+    }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kRedThreads) k_bsr_apply(Bsr<V> A, const double* __restrict__ x,
+                                                           double* __restrict__ y,
+                                                           const unsigned char* __restrict__ mask) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); a < A.rows; a += warps) {
+        double y0, y1, y2;
+        bsr_row<V, double, double>(A, x, a, lane, y0, y1, y2);
+        if (lane < 3) {
+            long long i = 3ll * a + lane;
+            double v = lane == 0 ? y0 : (lane == 1 ? y1 : y2);
+            if (mask && mask[i]) v = 0.0;
+            y[i] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------------------
+static int wait_scalars(nb2_ctx* c) {
+    NB2_CUDA(c, cudaMemcpyAsync(c->h_cgs, c->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost,
+                                c->stream));
+    NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    return NB2_OK;
+}
+
+constexpr int kChunk = 32;
+
+template <typename V, typename X>
+static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv, const double* b,
+                      double* xout, double tol, int maxit, bool use_mask, int* iterations,
+                      double* error, bool use_graphs, cudaGraphExec_t* cache) {
+    const int RB = reduction_blocks(c);
+    Bsr<V> A{c->brp, c->bcol, vals, c->N};
+    const long long n = c->n;
+    k_invdiag<V, X><<<(c->N + 255) / 256, 256, 0, c->stream>>>(A, inv);
+    k_init<X><<<RB, kRedThreads, 0, c->stream>>>(n, b, x, r, p, inv, c->cgs, c->partials, tol);
+    c->launches += 2;
+    // max_iterations is read by k_xr: set it with a tiny copy
+    NB2_CUDA(c, cudaMemcpyAsync(&c->cgs->max_iterations, &maxit, sizeof(int), cudaMemcpyHostToDevice,
+                                c->stream));
+    const unsigned char* mask = use_mask ? c->mask : nullptr;
+    auto enqueue = [&](int count) {
+        for (int it = 0; it < count; ++it) {
+            k_spmv<V, X><<<RB, kRedThreads, 0, c->stream>>>(A, p, q, mask, c->cgs, c->partials);
+            k_xr<X><<<RB, kRedThreads, 0, c->stream>>>(n, x, r, p, q, inv, c->cgs, c->partials);
+            k_p<X><<<RB, kRedThreads, 0, c->stream>>>(n, p, r, inv, c->cgs);
+        }
+    };
+    if (use_graphs && *cache == nullptr) {
+        // capture one block of iterations; fall back to plain launches if the stream cannot be
+        // captured (e.g. the legacy default stream)
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            enqueue(kChunk);
+            if (cudaStreamEndCapture(c->stream, &g) == cudaSuccess && g) {
+                if (cudaGraphInstantiate(cache, g, 0) != cudaSuccess) *cache = nullptr;
+                cudaGraphDestroy(g);
+            }
+        }
+        cudaGetLastError();
+        if (*cache == nullptr) use_graphs = false;
+    }
+    int guard = 0;
+    for (;;) {
+        if (use_graphs) {
+            NB2_CUDA(c, cudaGraphLaunch(*cache, c->stream));
+        } else {
+            enqueue(kChunk);
+        }
+        c->launches += 3 * kChunk;
+        int st = wait_scalars(c);
+        if (st) return st;
+        if (c->h_cgs->done) break;
+        if (++guard > (maxit / kChunk) + 4) break;  // scalars say not done: cannot happen
+    }
+    NB2_CUDA(c, cudaGetLastError());
+    k_copy_out<X><<<RB, kRedThreads, 0, c->stream>>>(n, x, xout);
+    c->launches++;
+    const CgScalars& h = *c->h_cgs;
+    *iterations = h.iterations;
+    *error = h.rhs_norm2 > 0 ? std::sqrt(h.rr / h.rhs_norm2) : 0.0;
+    if (h.status) return h.status;
+    if (!h.done) return NB2_E_TIMEOUT;
+    return NB2_OK;
+}
+
+int pcg_device_fp64(nb2_ctx* c, const double* b, double* x, double tol, int maxit, bool use_mask,
+                    int* iterations, double* error, bool use_graphs) {
+    return run_bsr_cg<double, double>(c, c->K64, c->cg_x, c->cg_r, c->cg_p, c->cg_q, c->cg_inv, b,
+                                      x, tol, maxit, use_mask, iterations, error,
+                                      use_graphs && use_mask, &c->graph64);
+}
+
+int pcg_device_fp32(nb2_ctx* c, const double* b, double* x, double tol, int maxit, int* iterations,
+                    double* error, bool use_graphs) {
+    return run_bsr_cg<float, float>(c, c->K32, c->cg32_x, c->cg32_r, c->cg32_p, c->cg32_q,
+                                    c->cg32_inv, b, x, tol, maxit, true, iterations, error,
+                                    use_graphs, &c->graph32);
+}
+
+void release_graphs(nb2_ctx* c) {
+    if (c->graph64) cudaGraphExecDestroy(c->graph64);
+    if (c->graph32) cudaGraphExecDestroy(c->graph32);
+    c->graph64 = c->graph32 = nullptr;
+}
+
+void bsr_spmv_fp64(nb2_ctx* c, const double* x, double* y, bool use_mask) {
+    Bsr<double> A{c->brp, c->bcol, c->K64, c->N};
+    k_bsr_apply<double><<<reduction_blocks(c), kRedThreads, 0, c->stream>>>(
+        A, x, y, use_mask ? c->mask : nullptr);
+    c->launches++;
+}
+
+void bsr_spmv_mixed_accum(nb2_ctx* c, const double* x, double* y) {
+    Bsr<float> A{c->brp, c->bcol, c->K32, c->N};
+    k_bsr_apply<float><<<reduction_blocks(c), kRedThreads, 0, c->stream>>>(A, x, y, nullptr);
+    c->launches++;
+}
+
+int compute_norms(nb2_ctx* c) {
+    k_norms<<<reduction_blocks(c), kRedThreads, 0, c->stream>>>(
+        c->n, c->du, c->u, c->rhs, c->fext, c->fint, c->partials, &c->cgs->counter[3], c->norms);
+    c->launches++;
+    NB2_CUDA(c, cudaMemcpyAsync(c->h_norms, c->norms, 5 * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+    NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    return NB2_OK;
+}
+
+// Standalone solve on a caller CSR (host buffers): own stream and buffers.
+int pcg_csr_host(int n, const int* rowptr, const int* col, const double* val, const double* b,
+                 double* x, double tol, int maxit, int* iterations, double* error,
+                 std::string* err) {
+    nb2_ctx tmp;
+    nb2_ctx* c = &tmp;
+    auto fail = [&](cudaError_t e) {
+        if (err) *err = cudaGetErrorString(e);
+        return NB2_E_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(e);
+    const long long nnz = rowptr[n];
+    int *rp = nullptr, *ci = nullptr;
+    double *v = nullptr, *bd = nullptr, *xd = nullptr, *r = nullptr, *p = nullptr, *q = nullptr,
+           *inv = nullptr, *xo = nullptr, *partials = nullptr;
+    CgScalars* s = nullptr;
+    CgScalars hs;
+    const int RB = 148 * 4;
+    int status = NB2_OK;
+#define TRY(call)                          \
+    if ((e = (call)) != cudaSuccess) {     \
+        status = fail(e);                  \
+        goto done;                         \
+    }
+    TRY(cudaMalloc(&rp, sizeof(int) * (n + 1)));
+    TRY(cudaMalloc(&ci, sizeof(int) * (nnz > 0 ? nnz : 1)));
+    TRY(cudaMalloc(&v, sizeof(double) * (nnz > 0 ? nnz : 1)));
+    TRY(cudaMalloc(&bd, sizeof(double) * n));
+    TRY(cudaMalloc(&xd, sizeof(double) * n));
+    TRY(cudaMalloc(&r, sizeof(double) * n));
+    TRY(cudaMalloc(&p, sizeof(double) * n));
+    TRY(cudaMalloc(&q, sizeof(double) * n));
+    TRY(cudaMalloc(&inv, sizeof(double) * n));
+    TRY(cudaMalloc(&xo, sizeof(double) * n));
+    TRY(cudaMalloc(&partials, sizeof(double) * RB * 8));
+    TRY(cudaMalloc(&s, sizeof(CgScalars)));
+    TRY(cudaMemsetAsync(s, 0, sizeof(CgScalars), c->stream));
+    TRY(cudaMemcpyAsync(rp, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c->stream));
+    TRY(cudaMemcpyAsync(ci, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, c->stream));
+    TRY(cudaMemcpyAsync(v, val, sizeof(double) * nnz, cudaMemcpyHostToDevice, c->stream));
+    TRY(cudaMemcpyAsync(bd, b, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    TRY(cudaMemcpyAsync(&s->max_iterations, &maxit, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    {
+        Csr A{rp, ci, v, n};
+        k_csr_invdiag<<<(n + 255) / 256, 256, 0, c->stream>>>(A, inv);
+        k_init<double><<<RB, kRedThreads, 0, c->stream>>>(n, bd, xd, r, p, inv, s, partials, tol);
+        TRY(cudaMemcpyAsync(&s->max_iterations, &maxit, sizeof(int), cudaMemcpyHostToDevice,
+                            c->stream));
+        int guard = 0;
+        for (;;) {
+            if (++guard > maxit / kChunk + 4) {
+                status = NB2_E_TIMEOUT;
+                goto done;
+            }
+            for (int it = 0; it < kChunk; ++it) {
+                k_csr_spmv<<<RB, kRedThreads, 0, c->stream>>>(A, p, q, s, partials);
+                k_xr<double><<<RB, kRedThreads, 0, c->stream>>>(n, xd, r, p, q, inv, s, partials);
+                k_p<double><<<RB, kRedThreads, 0, c->stream>>>(n, p, r, inv, s);
+            }
+            TRY(cudaMemcpyAsync(&hs, s, sizeof hs, cudaMemcpyDeviceToHost, c->stream));
+            TRY(cudaStreamSynchronize(c->stream));
+            if (hs.done) break;
+        }
+        TRY(cudaGetLastError());
+        TRY(cudaMemcpyAsync(x, xd, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+        TRY(cudaStreamSynchronize(c->stream));
+        *iterations = hs.iterations;
+        *error = hs.rhs_norm2 > 0 ? std::sqrt(hs.rr / hs.rhs_norm2) : 0.0;
+        if (hs.status) status = hs.status;
+    }
+done:
+#undef TRY
+    cudaFree(rp);
+    cudaFree(ci);
+    cudaFree(v);
+    cudaFree(bd);
+    cudaFree(xd);
+    cudaFree(r);
+    cudaFree(p);
+    cudaFree(q);
+    cudaFree(inv);
+    cudaFree(xo);
+    cudaFree(partials);
+    cudaFree(s);
+    cudaStreamDestroy(c->stream);
+    c->stream = nullptr;
+    return status;
+}
+
+}  // namespace nb2

@@ -1,0 +1,265 @@
+"""Problem description in neon's terms: material, constitutive model, Dirichlet boundaries,
+nodal forces, nonlinear / time / linear-solver options.
+
+The JSON keys follow neon's input schema (e.g. examples/solid_mechanics/hyperelastic/neohooke/
+cube/cube.json:1-72) so the same dictionaries drive the oracle and the device path.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from .mesh import Mesh, quad4_consistent_forces, structured_hex8, structured_tet4
+
+# Model identifiers of the C-ABI (include/neon_b200.h, enum nb2_model)
+LINEAR_ELASTIC, NEO_HOOKE, J2_SMALL_STRAIN, GAUSS_AFFINE_MICROSPHERE = 0, 1, 2, 3
+
+MODEL_NAMES = {
+    LINEAR_ELASTIC: "isotropic_linear_elasticity",
+    NEO_HOOKE: "neohooke",
+    J2_SMALL_STRAIN: "J2_plasticity",
+    GAUSS_AFFINE_MICROSPHERE: "microsphere",
+}
+
+
+@dataclasses.dataclass
+class Material:
+    """Isotropic parameters as neon stores them: bulk and shear modulus
+    (material/isotropic_elastic_property.cpp:10-43), yield stress and linear isotropic hardening
+    (material/isotropic_elastic_plastic.cpp:10-38), segments per chain
+    (material/micromechanical_elastomer.cpp:13-21)."""
+    model: int
+    K: float
+    G: float
+    yield_stress: float = 0.0
+    hardening: float = 0.0
+    segments_per_chain: float = 0.0
+
+    @property
+    def lam(self) -> float:
+        return self.K - 2.0 * self.G / 3.0
+
+    def params(self) -> np.ndarray:
+        return np.array([self.K, self.G, self.yield_stress, self.hardening,
+                         self.segments_per_chain], dtype=np.float64)
+
+
+def make_material(material: dict, constitutive: dict) -> Material:
+    """Restates the factory make_constitutive_model (constitutive_model_factory.cpp:26-161) for the
+    four models on the path, and the parameter parsing of isotropic_elastic_property."""
+    if "name" not in constitutive:
+        raise ValueError('Missing "name" in "constitutive"')
+    name = constitutive["name"]
+    if "bulk_modulus" in material and "shear_modulus" in material:
+        K, G = float(material["bulk_modulus"]), float(material["shear_modulus"])
+    elif "elastic_modulus" in material and "poissons_ratio" in material:
+        E, nu = float(material["elastic_modulus"]), float(material["poissons_ratio"])
+        if nu >= 0.5:
+            raise ValueError('"poissons_ratio" must be less than or equal to 0.5')
+        K = E / (3.0 * (1.0 - 2.0 * nu))
+        G = E / (2.0 * (1.0 + nu))
+    else:
+        raise ValueError('"elastic_modulus" and "poissons_ratio" or "bulk_modulus" and '
+                         '"shear_modulus" need to be specified as material properties')
+    if name in ("neohooke", "compressible_neohooke"):
+        return Material(NEO_HOOKE, K, G)
+    if name == "isotropic_linear_elasticity":
+        return Material(LINEAR_ELASTIC, K, G)
+    if name == "J2_plasticity":
+        if "finite_strain" not in constitutive:
+            raise ValueError('"small_strain_J2_plasticity" must have a boolean value for '
+                             '"finite_strain"')
+        if constitutive["finite_strain"]:
+            raise NotImplementedError("finite-strain J2 is not on this path")
+        if "yield_stress" not in material:
+            raise ValueError('"yield_stress" was not specified in material properties')
+        return Material(J2_SMALL_STRAIN, K, G, float(material["yield_stress"]),
+                        float(material.get("isotropic_hardening_modulus", 0.0)))
+    if name == "microsphere":
+        for key, msg in (("type", 'Missing "type" as "affine" or "nonaffine" in microsphere model'),
+                         ("quadrature", 'Missing "quadrature" as "BO21", "BO33" or "FM900" in '
+                                        'microsphere model')):
+            if key not in constitutive:
+                raise ValueError(msg)
+        if constitutive["type"] != "affine" or constitutive.get("statistics") != "gaussian" \
+                or constitutive["quadrature"] != "BO21" or "ageing" in constitutive:
+            raise NotImplementedError("only the Gaussian affine BO21 microsphere is on this path")
+        if "segments_per_chain" not in material:
+            raise ValueError("segments_per_chain not specified in material data")
+        return Material(GAUSS_AFFINE_MICROSPHERE, K, G,
+                        segments_per_chain=float(material["segments_per_chain"]))
+    raise ValueError(f"The model name {name} is not recognised")
+
+
+@dataclasses.dataclass
+class DofTable:
+    """A Dirichlet boundary (nodal_value, mesh/boundary/nodal_value.cpp) or a nodal force: DOFs
+    and a time/value table interpolated linearly (mesh/boundary/boundary.cpp:55-85).  For forces,
+    ``weights`` scales the value per DOF (consistent forces of a unit traction)."""
+    dofs: np.ndarray
+    times: np.ndarray
+    values: np.ndarray
+    weights: np.ndarray | None = None
+    name: str = ""
+
+
+def sinusoidal_table(amplitude, period, number_of_cycles, phase, generate_time_step):
+    """boundary::generate_sinusoidal (mesh/boundary/boundary.cpp:87-147) for one block."""
+    omega = 2.0 * math.pi / period
+    steps = int(number_of_cycles * period / generate_time_step)
+    block = np.arange(1, steps + 1, dtype=np.float64)
+    scale = number_of_cycles * period / block[-1]
+    t = block * scale + 0.0
+    v = amplitude * np.sin(omega * t + phase)
+    return np.concatenate([[0.0], t]), np.concatenate([[0.0], v])
+
+
+def dirichlet_boundaries(mesh: Mesh, boundaries: list, generate_time_step: float = 1.0):
+    """mesh<submesh>::allocate_displacement_boundary (mesh/mechanics/solid/mesh.cpp:116-143).
+
+    Returns DofTables in the order static_matrix iterates them: boundary names sorted (std::map),
+    and within a name the components x, y, z (the dof_table map)."""
+    out = []
+    for b in sorted(boundaries, key=lambda b: b["name"]):
+        if b.get("type", "displacement") != "displacement":
+            continue
+        nodes = mesh.boundary_nodes(b["name"])
+        for comp, key in enumerate("xyz"):
+            if key not in b:
+                continue
+            if b.get("generate_type") == "sinusoidal":
+                t, v = sinusoidal_table(b[key][0], b["period"][0], b["number_of_cycles"][0],
+                                        b["phase"][0], generate_time_step)
+            else:
+                t, v = np.asarray(b["time"], float), np.asarray(b[key], float)
+            out.append(DofTable((3 * nodes + comp).astype(np.int32), t, v, name=b["name"]))
+    return out
+
+
+@dataclasses.dataclass
+class Options:
+    """nonlinear_options (static_matrix.hpp:109-143), time/increments
+    (solver/adaptive_time_step.cpp:12-165) and linear_solver (linear_solver_factory.cpp:27-65)."""
+    residual_tolerance: float = 1e-3
+    displacement_tolerance: float = 1e-3
+    linear_iterations: int = 10
+    absolute_tolerance: bool = False
+    period: float = 1.0
+    initial: float = 1.0
+    minimum: float = 1.0
+    maximum: float = 1.0
+    adaptive: bool = False
+    cg_tolerance: float = 1e-5
+    cg_maximum_iterations: int = 2000
+    use_rcm: bool = True
+
+
+@dataclasses.dataclass
+class Problem:
+    name: str
+    mesh: Mesh
+    material: Material
+    dirichlet: list
+    options: Options
+    nodal_forces: list = dataclasses.field(default_factory=list)
+    element_shear_modulus: np.ndarray | None = None
+
+    @property
+    def ndofs(self) -> int:
+        return 3 * self.mesh.num_nodes
+
+
+def _rollers(extra):
+    b = [{"name": "x0", "type": "displacement", "time": [0.0, 1.0], "x": [0.0, 0.0]},
+         {"name": "y0", "type": "displacement", "time": [0.0, 1.0], "y": [0.0, 0.0]},
+         {"name": "bottom", "type": "displacement", "time": [0.0, 1.0], "z": [0.0, 0.0]}]
+    return b + extra
+
+
+def config_c1(n: int = 20) -> Problem:
+    """Small-strain isotropic linear elasticity, E=200e3, nu=0.3, unit cube n^3 hex8, z=0 fully
+    fixed, uz=1e-3 on z=1, one increment, Jacobi-PCG rtol 1e-10."""
+    mesh = structured_hex8(n)
+    mat = make_material({"elastic_modulus": 200e3, "poissons_ratio": 0.3},
+                        {"name": "isotropic_linear_elasticity"})
+    bcs = [{"name": "bottom", "time": [0.0, 1.0], "x": [0.0, 0.0], "y": [0.0, 0.0],
+            "z": [0.0, 0.0]},
+           {"name": "top", "time": [0.0, 1.0], "z": [0.0, 1e-3]}]
+    opts = Options(residual_tolerance=1e-6, displacement_tolerance=1e-6, linear_iterations=10,
+                   period=1.0, initial=1.0, minimum=1.0, maximum=1.0, adaptive=False,
+                   cg_tolerance=1e-10, cg_maximum_iterations=100000)
+    return Problem("c1_linear_elastic_hex8_%d" % n, mesh, mat, dirichlet_boundaries(mesh, bcs), opts)
+
+
+def config_c2(n: int = 64, seed: int = 20240601, increments: int = 10) -> Problem:
+    """Compressible neo-Hooke (mu=1, K=10), n^3 hex8 with interior nodes jittered by U(+-0.1h)
+    (PCG64 seed), symmetry rollers on x=0/y=0/z=0, top stretch to 1.3 in equal increments."""
+    mesh = structured_hex8(n, jitter=0.1, seed=seed)
+    mat = make_material({"shear_modulus": 1.0, "bulk_modulus": 10.0}, {"name": "neohooke"})
+    bcs = _rollers([{"name": "top", "type": "displacement", "time": [0.0, 1.0], "z": [0.0, 0.3]}])
+    dt = 1.0 / increments
+    opts = Options(residual_tolerance=1e-8, displacement_tolerance=1e-8, linear_iterations=15,
+                   period=1.0, initial=dt, minimum=dt, maximum=dt, adaptive=False,
+                   cg_tolerance=1e-10, cg_maximum_iterations=200000)
+    return Problem("c2_neohooke_hex8_%d" % n, mesh, mat, dirichlet_boundaries(mesh, bcs), opts)
+
+
+def config_c3(n: int = 100, steps: int = 20) -> Problem:
+    """Small-strain J2 plasticity with linear isotropic hardening (E=200e3, nu=0.3, sigma_y=200,
+    H=1e3), n^3 hex8, bottom clamped, top uz = 5e-3 sin(2 pi t / steps) sampled at every unit of
+    time (one cycle, +-5e-3) -- neon's sinusoidal generator with period = steps."""
+    mesh = structured_hex8(n)
+    mat = make_material({"elastic_modulus": 200e3, "poissons_ratio": 0.3, "yield_stress": 200.0,
+                         "isotropic_hardening_modulus": 1e3},
+                        {"name": "J2_plasticity", "finite_strain": False})
+    bcs = [{"name": "bottom", "time": [0.0, float(steps)], "x": [0.0, 0.0], "y": [0.0, 0.0],
+            "z": [0.0, 0.0]},
+           {"name": "top", "generate_type": "sinusoidal", "z": [5e-3], "period": [float(steps)],
+            "phase": [0.0], "number_of_cycles": [1.0]}]
+    opts = Options(residual_tolerance=1e-8, displacement_tolerance=1e-8, linear_iterations=15,
+                   period=float(steps), initial=1.0, minimum=1.0, maximum=1.0, adaptive=False,
+                   cg_tolerance=1e-10, cg_maximum_iterations=200000)
+    return Problem("c3_j2_hex8_%d" % n, mesh, mat, dirichlet_boundaries(mesh, bcs, 1.0), opts)
+
+
+def config_c4(n: int = 48, seed_field: int = 7, traction: float = 0.05) -> Problem:
+    """Gaussian affine microsphere (BO21, K=100, G=1 scaled by a per-element lognormal(0, 0.3)
+    field), n^3 hex8, bottom clamped, uniform top traction in z (consistent quad4 forces)."""
+    mesh = structured_hex8(n)
+    mat = make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0, "segments_per_chain": 50},
+                        {"name": "microsphere", "type": "affine", "statistics": "gaussian",
+                         "quadrature": "BO21"})
+    rng = np.random.Generator(np.random.PCG64(seed_field))
+    Ge = rng.lognormal(mean=0.0, sigma=0.3, size=mesh.num_elements) * mat.G
+    bcs = [{"name": "bottom", "time": [0.0, 1.0], "x": [0.0, 0.0], "y": [0.0, 0.0],
+            "z": [0.0, 0.0]}]
+    dofs, w = quad4_consistent_forces(mesh, "top", (0.0, 0.0, 1.0))
+    nf = [DofTable(dofs, np.array([0.0, 1.0]), np.array([0.0, traction]), weights=w, name="top")]
+    opts = Options(residual_tolerance=1e-9, displacement_tolerance=1e-9, linear_iterations=15,
+                   period=1.0, initial=1.0, minimum=1.0, maximum=1.0, adaptive=False,
+                   cg_tolerance=1e-10, cg_maximum_iterations=200000)
+    return Problem("c4_microsphere_hex8_%d" % n, mesh, mat, dirichlet_boundaries(mesh, bcs), opts,
+                   nodal_forces=nf, element_shear_modulus=Ge)
+
+
+def config_c5_instance(m: int, mu: float, increments: int = 5) -> Problem:
+    """One instance of the batched set: m^3 cubes x 6 tet4, neo-Hooke mu, K = 20 mu, rollers +
+    top stretch 1.1 in equal increments."""
+    mesh = structured_tet4(m)
+    mat = make_material({"shear_modulus": mu, "bulk_modulus": 20.0 * mu}, {"name": "neohooke"})
+    bcs = _rollers([{"name": "top", "type": "displacement", "time": [0.0, 1.0], "z": [0.0, 0.1]}])
+    dt = 1.0 / increments
+    opts = Options(residual_tolerance=1e-8, displacement_tolerance=1e-8, linear_iterations=15,
+                   period=1.0, initial=dt, minimum=dt, maximum=dt, adaptive=False,
+                   cg_tolerance=1e-10, cg_maximum_iterations=200000)
+    return Problem("c5_neohooke_tet4_%d" % m, mesh, mat, dirichlet_boundaries(mesh, bcs), opts)
+
+
+def config_c5_sizes(count: int = 256, seed: int = 11, lo: int = 8, hi: int = 40):
+    """Seeded (cells per side, mu) pairs of the batched workload."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    m = rng.integers(lo, hi + 1, size=count)
+    mu = rng.uniform(0.5, 2.0, size=count)
+    return [(int(a), float(b)) for a, b in zip(m, mu)]
