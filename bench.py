@@ -209,10 +209,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=100)
-    ap.add_argument("--newton-load-steps", type=int, default=1)
+    ap.add_argument("--newton-load-steps", type=int, default=4)
     ap.add_argument("--no-newton", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cg-iterations", type=int, default=200)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -311,12 +313,79 @@ def main():
                 "peak_source": hbm_src, "algorithmic_bytes": alg_bytes,
                 "algorithmic_flops": alg_flops}
 
-    # end to end through the drop-in C-ABI with host buffers (copies inside the timed region)
+    pcg = None
+    if args.cg_iterations > 0:
+        pcg = pcg_timing(api, torch, stream, mesh, pr, args.cg_iterations, hbm)
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(api, args, pr, u, world, dist, torch, E)
+
+    newton = None
+    if not args.no_newton:
+        newton = newton_comparison(api, P, args, mesh)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample()
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": warmup, "ms_per_step": t_max * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"J2 hex8 {args.size}^3 (sigma_y=200, E=200e3, nu=0.3, "
+                                   f"H=1e3), fused update+K+f_int, plastic state",
+                       "elements": E, "dofs": mesh.ndofs, "nnz": mesh.nnz,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (K 1.96 GB, state 0.45 GB)"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "timed_region_ms": region_ms, "clocks": clock_info,
+            "fp32_fma_peak_tflops": fp32_peak / 1e12, "pcg": pcg, "newton": newton}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    mesh.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def pcg_timing(api, torch, stream, mesh, pr, iters, hbm):
+    """Per-iteration device time of the PCG on the full K (FP64 and FP32), and its bandwidth
+    against the algorithmic bytes of one iteration."""
+    dofs = np.concatenate([t.dofs for t in pr.dirichlet if t.name == "bottom"])
+    mesh.set_dirichlet_mask(dofs)
+    n, nnz, nnzb, N = mesh.ndofs, mesh.nnz, mesh.nnzb, pr.mesh.num_nodes
+    out = {}
+    for name, prec in (("fp64", api.FP64), ("fp32", api.MIXED)):
+        if prec == api.MIXED:
+            mesh.save_internal_variables(False)
+            mesh.update_assemble_device(api.MIXED)
+        sv = 8 if prec == api.FP64 else 4
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        times = {}
+        for its in (20, iters + 20):
+            mesh.solve_device(prec, 0.0, its)  # warm (graph capture on first use)
+            e0.record(stream)
+            mesh.solve_device(prec, 0.0, its)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times[its] = e0.elapsed_time(e1)
+        ms = (times[iters + 20] - times[20]) / iters
+        # matrix values + block columns + block row pointers, 13 vector streams, Dirichlet mask
+        alg = sv * nnz + 4 * nnzb + 4 * (N + 1) + 13 * sv * n + n
+        out[name] = {"ms_per_iteration": ms, "algorithmic_bytes": alg,
+                     "achieved_gbs": alg / (ms * 1e-3) / 1e9,
+                     "frac_of_hbm": alg / (ms * 1e-3) / 1e9 / hbm}
+    out["fp32_over_fp64_speedup"] = out["fp64"]["ms_per_iteration"] / out["fp32"]["ms_per_iteration"]
+    return out
+
+
+def end_to_end(api, args, pr, u, world, dist, torch, E):
+    """The metric through the drop-in C-ABI with host buffers, copies inside the timed region."""
     mesh_e2e = api.SolidMesh(pr.mesh.X, pr.mesh.conn, pr.material)
     mesh_e2e.save_internal_variables(True)
     Kh = np.zeros(mesh_e2e.nnz)
     fh = np.zeros(mesh_e2e.ndofs)
-    import ctypes
     L = api.lib()
 
     def e2e_step():
@@ -338,42 +407,16 @@ def main():
            "call": "nb2_update_internal_variables + nb2_assemble (host u in, host CSR K + f_int "
                    "out)"}
     mesh_e2e.close()
-
-    newton = None
-    if not args.no_newton:
-        newton = newton_comparison(api, P, args, mesh)
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline_sample()
-
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": warmup, "ms_per_step": t_max * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"J2 hex8 {args.size}^3 (sigma_y=200, E=200e3, nu=0.3, "
-                                   f"H=1e3), fused update+K+f_int, plastic state",
-                       "elements": E, "dofs": mesh.ndofs, "nnz": mesh.nnz,
-                       "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (K 1.96 GB, state 0.45 GB)"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "timed_region_ms": region_ms, "clocks": clock_info,
-            "fp32_fma_peak_tflops": fp32_peak / 1e12, "newton": newton}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    mesh.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-    return 0
+    return e2e
 
 
 def newton_comparison(api, P, args, mesh_unused):
     """FP64 vs mixed device Newton on the first load increment(s) of the cyclic J2 history."""
     pr = P.config_c3(args.size)
-    pr.options.period = float(args.newton_load_steps)
+    pr.options.period = float(args.newton_load_steps) * pr.options.initial
     out = {}
     sols = {}
-    for name, prec, tol in (("fp64", api.FP64, None), ("mixed", api.MIXED, 1e-5)):
+    for name, prec, tol in (("fp64", api.FP64, None), ("mixed", api.MIXED, 1e-4)):
         sm = api.StaticMatrix(pr, precision=prec, mixed_inner_tolerance=tol or 1e-6)
         try:
             u = sm.solve(raise_on_error=False)

@@ -221,6 +221,14 @@ int nb2_update_assemble_device(nb2_ctx* ctx, int32_t precision);
 /* Copy device K (CSR order, FP64 path) / f_int to host. */
 int nb2_download_system(nb2_ctx* ctx, double* K_values, double* f_int);
 int nb2_synchronize(nb2_ctx* ctx);
+/* Mark DOFs as active Dirichlet DOFs of the device solve (rows/columns treated as zeroed, the
+ * enforce_dirichlet_conditions semantics of static_matrix.hpp:279-320). */
+int nb2_set_dirichlet_mask(nb2_ctx* ctx, const int32_t* dofs, int32_t num_dofs);
+/* Device PCG on the resident K (precision NB2_FP64: FP64 K; NB2_MIXED: FP32 K with FP64 dots)
+ * with the context's internal force as right-hand side (masked DOFs zeroed), from x0 = 0.
+ * tolerance 0 runs exactly maximum_iterations iterations (timing). */
+int nb2_solve_device(nb2_ctx* ctx, int32_t precision, double tolerance, int32_t maximum_iterations,
+                     int32_t* iterations, double* error);
 
 #ifdef __cplusplus
 }

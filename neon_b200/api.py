@@ -109,6 +109,9 @@ _SIGS = {
     "nb2_update_assemble_device": (C.c_int, [P, C.c_int32]),
     "nb2_download_system": (C.c_int, [P, P, P]),
     "nb2_synchronize": (C.c_int, [P]),
+    "nb2_set_dirichlet_mask": (C.c_int, [P, P, C.c_int32]),
+    "nb2_solve_device": (C.c_int, [P, C.c_int32, C.c_double, C.c_int32, C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_double)]),
     "nb2_probe_fma_throughput": (C.c_int, [C.c_int32, C.POINTER(C.c_double)]),
 }
 
@@ -239,6 +242,18 @@ class SolidMesh:
 
     def synchronize(self):
         _check(lib().nb2_synchronize(self.h), self.h, "synchronize")
+
+    def set_dirichlet_mask(self, dofs):
+        dofs = np.ascontiguousarray(dofs, dtype=np.int32)
+        _check(lib().nb2_set_dirichlet_mask(self.h, dofs.ctypes.data, len(dofs)), self.h, "mask")
+
+    def solve_device(self, precision=FP64, tolerance=0.0, maximum_iterations=100):
+        it = C.c_int32()
+        err = C.c_double()
+        _check(lib().nb2_solve_device(self.h, int(precision), float(tolerance),
+                                      int(maximum_iterations), C.byref(it), C.byref(err)),
+               self.h, "solve_device")
+        return it.value, err.value
 
     def set_stream(self, stream_handle: int):
         _check(lib().nb2_set_stream(self.h, stream_handle), self.h, "set_stream")

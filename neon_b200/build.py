@@ -38,6 +38,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     deps = [os.path.join(CSRC, s) for s in SOURCES] + [
         os.path.join(CSRC, "nb2_internal.cuh"), os.path.join(CSRC, "host_driver.hpp"),
+        os.path.join(CSRC, "element_kernel.cuh"),
         os.path.join(ROOT, "include", "neon_b200.h"),
         os.path.join(ROOT, "include", "neon_b200_probe.h")]
     if not force and not _stale(LIB, deps):
@@ -61,6 +62,24 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     return LIB
 
 
+DRIVER = os.path.join(LIBDIR, "adapter_driver")
+
+
+def build_adapter_driver(force: bool = False) -> str:
+    """C++ consumer of include/neon_b200.hpp (tests/cpp/adapter_driver.cpp), linked against the
+    library with an $ORIGIN rpath so it runs from the tree."""
+    lib = build()
+    src = os.path.join(ROOT, "tests", "cpp", "adapter_driver.cpp")
+    deps = [src, lib, os.path.join(ROOT, "include", "neon_b200.hpp")]
+    if force or _stale(DRIVER, deps):
+        cmd = [shutil.which("g++") or "g++", "-std=c++17", "-O2", src, "-o", DRIVER,
+               "-I" + os.path.join(ROOT, "include"), "-L" + LIBDIR, "-lneon_b200",
+               "-Wl,-rpath,$ORIGIN"]
+        subprocess.run(cmd, check=True)
+    return DRIVER
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose_ptxas="--verbose-ptxas" in sys.argv)
+    build_adapter_driver(force="--force" in sys.argv)
     print(LIB)

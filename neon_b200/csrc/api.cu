@@ -126,7 +126,8 @@ static int ensure_split_buffers(nb2_ctx* c) {
 
 static int ensure_k32(nb2_ctx* c) {
     if (c->K32) return NB2_OK;
-    NB2_TRY(dev_alloc(c, &c->K32, 9 * c->nnzb));
+    // +16 B: the bulk SpMV widens every copy to 16-byte boundaries
+    NB2_TRY(dev_alloc(c, &c->K32, 9 * c->nnzb + 4));
     NB2_TRY(dev_alloc(c, &c->cg32_x, (long long)c->n));
     NB2_TRY(dev_alloc(c, &c->cg32_r, (long long)c->n));
     NB2_TRY(dev_alloc(c, &c->cg32_p, (long long)c->n));
@@ -137,7 +138,7 @@ static int ensure_k32(nb2_ctx* c) {
 
 static int ensure_k64(nb2_ctx* c) {
     if (c->K64) return NB2_OK;
-    return dev_alloc(c, &c->K64, 9 * c->nnzb);
+    return dev_alloc(c, &c->K64, 9 * c->nnzb + 2);  // +16 B for the bulk SpMV spans
 }
 
 extern "C" {
@@ -467,6 +468,45 @@ int nb2_synchronize(nb2_ctx* c) {
     return NB2_OK;
 }
 
+int nb2_set_dirichlet_mask(nb2_ctx* c, const int32_t* dofs, int32_t nd) {
+    if (!c || (nd > 0 && !dofs)) return NB2_E_INPUT;
+    for (int i = 0; i < nd; ++i)
+        if (dofs[i] < 0 || dofs[i] >= c->n) return NB2_E_INPUT;
+    NB2_CUDA(c, cudaMemsetAsync(c->mask, 0, c->n, c->stream));
+    if (nd > 0) {
+        int* d = nullptr;
+        NB2_CUDA(c, cudaMallocAsync(&d, sizeof(int) * nd, c->stream));
+        NB2_CUDA(c, cudaMemcpyAsync(d, dofs, sizeof(int) * nd, cudaMemcpyHostToDevice, c->stream));
+        k_scatter_mask<<<(nd + 255) / 256, 256, 0, c->stream>>>(nd, d, c->mask);
+        c->launches++;
+        NB2_CUDA(c, cudaFreeAsync(d, c->stream));
+    }
+    NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    return NB2_OK;
+}
+
+int nb2_solve_device(nb2_ctx* c, int32_t precision, double tol, int32_t maxit, int32_t* iterations,
+                     double* error) {
+    if (!c || maxit <= 0) return NB2_E_INPUT;
+    if ((precision == NB2_FP64 && !c->K64) || (precision != NB2_FP64 && !c->K32)) {
+        c->error = "nb2_solve_device needs an assembled K of that precision";
+        return NB2_E_INPUT;
+    }
+    NB2_CUDA(c, cudaMemcpyAsync(c->rhs, c->fint, sizeof(double) * c->n, cudaMemcpyDeviceToDevice,
+                                c->stream));
+    k_zero_masked<<<grid_for(c->n), 256, 0, c->stream>>>(c->n, c->mask, c->rhs);
+    c->launches++;
+    int it = 0;
+    double err = 0;
+    int st = precision == NB2_FP64
+                 ? pcg_device_fp64(c, c->rhs, c->du, tol, maxit, true, &it, &err, true)
+                 : pcg_device_fp32(c, c->rhs, c->du, tol, maxit, &it, &err, true);
+    if (iterations) *iterations = it;
+    if (error) *error = err;
+    if (st == NB2_E_CG_MAXIT && tol == 0.0) st = NB2_OK;  // fixed-count timing run
+    return st;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------------
@@ -502,6 +542,8 @@ struct Newton {
             }
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (double* p : {rlin, corr, yvec})
+            if (p) cudaFree(p);
     }
 
     int upload(const nb2_dof_table* in, int count, std::vector<DeviceTable>& out, bool weighted) {
@@ -540,12 +582,25 @@ struct Newton {
 
     unsigned grid() const { return grid_for(c->n); }
 
-    // update (+ assemble) at the context displacement
+    double *rlin = nullptr, *corr = nullptr, *yvec = nullptr;  // mixed defect correction
+
+    int alloc_mixed() {
+        NB2_CUDA(c, cudaMalloc(&rlin, sizeof(double) * c->n));
+        NB2_CUDA(c, cudaMalloc(&corr, sizeof(double) * c->n));
+        NB2_CUDA(c, cudaMalloc(&yvec, sizeof(double) * c->n));
+        return NB2_OK;
+    }
+
+    bool mixed() const { return o.precision == NB2_MIXED; }
+
+    // update (+ assemble) at the context displacement; the mixed path also stores the FP64
+    // tangent coefficients for its matrix-free defect residual
     int element_pass(bool assemble) {
         NB2_TRY(reset_status(c));
         time_begin();
         int mode = MODE_CONSTITUTIVE | MODE_FORCE | (assemble ? MODE_STIFFNESS : 0);
-        NB2_TRY(launch_element_kernel(c, mode, o.precision == NB2_MIXED ? NB2_MIXED : NB2_FP64));
+        if (mixed() && assemble) mode |= MODE_STORE;
+        NB2_TRY(launch_element_kernel(c, mode, mixed() ? NB2_MIXED : NB2_FP64));
         t_elem += time_end();
         return read_status(c);
     }
@@ -583,8 +638,8 @@ struct Newton {
             c->launches++;
         }
         double* tmp = c->cg_q;  // free until the solve
-        if (o.precision == NB2_MIXED)
-            bsr_spmv_mixed_accum(c, c->inc, tmp);
+        if (mixed())
+            NB2_TRY(launch_apply(c, c->inc, tmp));  // FP64 tangent, matrix-free
         else
             bsr_spmv_fp64(c, c->inc, tmp, false);
         k_axpy<<<grid(), 256, 0, c->stream>>>(c->n, -1.0, tmp, c->rhs);
@@ -605,14 +660,49 @@ struct Newton {
         }
     }
 
+    // Mixed precision: FP64 defect correction around FP32 inner PCG solves.  The defect
+    // rlin = rhs - K du uses the FP64 tangent (matrix-free), so du converges to the solution of
+    // the same FP64 system as the FP64 path, to the same relative tolerance.
+    int solve_mixed(int* iterations) {
+        const double b2 = device_dot_sync(c, c->rhs, c->rhs, c->n);
+        const double thr = std::max(o.cg_tolerance * o.cg_tolerance * b2, 2.2250738585072014e-308);
+        NB2_CUDA(c, cudaMemsetAsync(c->du, 0, sizeof(double) * c->n, c->stream));
+        NB2_CUDA(c, cudaMemcpyAsync(rlin, c->rhs, sizeof(double) * c->n, cudaMemcpyDeviceToDevice,
+                                    c->stream));
+        int total = 0;
+        double r2 = b2;
+        for (int ref = 0; ref < 30 && r2 >= thr && b2 > 0; ++ref) {
+            int it = 0;
+            double err = 0;
+            int st = pcg_device_fp32(c, rlin, corr, o.mixed_inner_tolerance,
+                                     std::max(1, o.cg_maximum_iterations - total), &it, &err,
+                                     o.use_graphs != 0);
+            total += it;
+            if (st && st != NB2_E_CG_MAXIT) {
+                *iterations = total;
+                return st;
+            }
+            k_axpy<<<grid(), 256, 0, c->stream>>>(c->n, 1.0, corr, c->du);
+            NB2_TRY(launch_apply(c, c->du, yvec));
+            k_sub<<<grid(), 256, 0, c->stream>>>(c->n, c->rhs, yvec, rlin);
+            k_zero_masked<<<grid(), 256, 0, c->stream>>>(c->n, c->mask, rlin);
+            c->launches += 3;
+            r2 = device_dot_sync(c, rlin, rlin, c->n);
+            if (total >= o.cg_maximum_iterations) break;
+        }
+        *iterations = total;
+        if (!std::isfinite(r2)) return NB2_E_NAN;
+        if (r2 >= thr && b2 > 0) return NB2_E_CG_MAXIT;
+        return NB2_OK;
+    }
+
     int solve_linear() {
         int it = 0;
         double err = 0;
         time_begin();
         int st;
-        if (o.precision == NB2_MIXED)
-            st = pcg_device_fp32(c, c->rhs, c->du, o.mixed_inner_tolerance, o.cg_maximum_iterations,
-                                 &it, &err, o.use_graphs != 0);
+        if (mixed())
+            st = solve_mixed(&it);
         else
             st = pcg_device_fp64(c, c->rhs, c->du, o.cg_tolerance, o.cg_maximum_iterations, true,
                                  &it, &err, o.use_graphs != 0);
@@ -714,7 +804,9 @@ extern "C" int nb2_static_solve(nb2_ctx* c, const nb2_solver_options* options,
     if (nw.o.linear_iterations <= 0 || nw.o.cg_maximum_iterations <= 0) return NB2_E_INPUT;
     if (nw.o.precision == NB2_MIXED) {
         NB2_TRY(ensure_k32(c));
-        if (!(nw.o.mixed_inner_tolerance > 0)) nw.o.mixed_inner_tolerance = 1e-6;
+        NB2_TRY(ensure_split_buffers(c));
+        NB2_TRY(nw.alloc_mixed());
+        if (!(nw.o.mixed_inner_tolerance > 0)) nw.o.mixed_inner_tolerance = 1e-4;
     } else {
         NB2_TRY(ensure_k64(c));
     }

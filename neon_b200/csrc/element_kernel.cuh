@@ -1,0 +1,333 @@
+// element_kernel.cuh -- the fused element kernel (included by elements.cu).
+//
+// A group of G lanes owns one element (hex8: 8 lanes, 4 elements per warp; tet4: 2 lanes).
+//   phase 0  gather node coordinates (X, x = u + X) into shared memory;
+//   phase 1  lane l runs quadrature point l in FP64 (deformation measures, det F check,
+//            constitutive update, current gradient L = dN J^-1, tangent coefficients); the
+//            internal force of every node is reduced over the group with shuffles;
+//   phase 2  each lane accumulates its upper-triangular 3x3 blocks over the points in Real
+//            precision, in two passes of at most 3 blocks (fewer live registers), and adds
+//            them (and their mirrored blocks) to K with red.global.add.
+// Shared memory per element holds L (Real) for every point, the flow direction N (J2) and,
+// for finite-strain models, g = s sigma L (FP64) used by the geometric stiffness.
+#pragma once
+
+template <int NPE, int MODEL, typename Real, int MODE>
+__global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : 8) k_element(ElementArgs A) {
+    using T = Topo<NPE>;
+    constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC, MAXB = T::MAXB;
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
+    constexpr bool kJ2 = (MODEL == MODEL_J2);
+    constexpr bool kCon = (MODE & MODE_CONSTITUTIVE) != 0;
+    constexpr bool kStiff = (MODE & MODE_STIFFNESS) != 0;
+    constexpr bool kForce = (MODE & MODE_FORCE) != 0;
+    constexpr bool kStore = (MODE & MODE_STORE) != 0;
+    constexpr int LS = NQ * NPE * 3 + 2;           // per-element stride of L (padded)
+    constexpr int NS = kJ2 ? NQ * 6 + 2 : 1;       // flow directions
+    constexpr int GS = kFinite ? NQ * NPE * 3 + 1 : 1;  // g = s sigma L
+    constexpr int NG = (NPE + G - 1) / G;          // nodes per lane
+
+    __shared__ double sX[EPC][NPE][3];
+    __shared__ double sx[EPC][NPE][3];
+    __shared__ double sdN[NQ][NPE][3];
+    __shared__ Real sL[EPC][LS];
+    __shared__ Real sN[EPC][NS];
+    __shared__ double sG[EPC][GS];
+    __shared__ Real sC[EPC][NQ][4];
+
+    const int tid = threadIdx.x;
+    const int le = tid / G;
+    const int lane = tid % G;
+    const long long e = (long long)blockIdx.x * EPC + le;
+    const bool valid = e < A.E;
+
+    for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
+        (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
+
+    // phase 0
+    int node[NG];
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+        const int a = lane + j * G;
+        node[j] = 0;
+        if (a < NPE && valid) {
+            const int nd = A.conn[e * NPE + a];
+            node[j] = nd;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double Xv = A.X[3ll * nd + k];
+                sX[le][a][k] = Xv;
+                sx[le][a][k] = A.u[3ll * nd + k] + Xv;
+            }
+        }
+    }
+    __syncthreads();
+
+    // phase 1
+    double fown[NG][3];
+#pragma unroll
+    for (int j = 0; j < NG; ++j) fown[j][0] = fown[j][1] = fown[j][2] = 0.0;
+    {
+        const int l = lane;
+        const bool active = valid && l < NQ;
+        QpOut o;
+        o.lam = o.mu = o.b = 0.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) o.sig[c] = o.N[c] = 0.0;
+        double Ji[9], s = 0.0;
+        if (active) {
+            const double w = (NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0);
+            const long long q = e * NQ + l;
+            // one pass over the nodes: F = x dN, F0 = X dN and U = (x - X) dN; then
+            // H = U F0^-1 (= sum_a (x_a - X_a) (x) (dN_a F0^-1), submesh.cpp:225-231)
+            double Fc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            double F0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            double U[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const double xi = sx[le][a][i], Xi = sX[le][a][i], di = xi - Xi;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const double d = sdN[l][a][k];
+                        Fc[i * 3 + k] += xi * d;
+                        if constexpr (kCon) {
+                            F0[i * 3 + k] += Xi * d;
+                            U[i * 3 + k] += di * d;
+                        }
+                    }
+                }
+            if constexpr (kCon) {
+                double F0i[9];
+                inv3(F0, F0i);
+                double Hm[9];
+                matmul3(U, F0i, Hm);
+                double Fd[9];
+                matmul3(Fc, F0i, Fd);
+                const double detF = det3(Fd);
+                if (signbit(detF)) {
+                    const unsigned long long key = ((unsigned long long)q << 32) |
+                                                   (unsigned long long)__float_as_uint((float)detF);
+                    atomicMin(&A.status->negdet_first, key);
+                    atomicAdd(&A.status->negdet_count, 1u);
+                    report_status(A.status, NB2_E_NEG_DETJ);
+                }
+                if constexpr (MODEL == MODEL_LE) {
+                    cm_linear_elastic(A, Hm, o);
+                } else if constexpr (MODEL == MODEL_NH) {
+                    cm_neo_hooke(A, Fd, detF, o);
+                } else if constexpr (MODEL == MODEL_J2) {
+                    if (!cm_j2(A, q, Hm, o)) report_status(A.status, NB2_E_RETURN_MAP);
+                } else {
+                    cm_microsphere(A, A.Ge ? A.Ge[e] : A.G, Fd, detF, o);
+                }
+                bool bad = isnan(o.lam) || isnan(o.mu);
+#pragma unroll
+                for (int c = 0; c < 6; ++c) bad |= isnan(o.sig[c]);
+                if (bad) report_status(A.status, NB2_E_NAN);
+                if constexpr (kStore) {
+                    const long long n = A.nqp;
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) A.sig[c * n + q] = o.sig[c];
+                    A.dpar[0 * n + q] = o.lam;
+                    A.dpar[1 * n + q] = o.mu;
+                    A.dpar[2 * n + q] = o.b;
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) A.dpar[(3 + c) * n + q] = kJ2 ? o.N[c] : 0.0;
+                    A.detF[q] = detF;
+                }
+            } else {
+                const long long n = A.nqp;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) o.sig[c] = A.sig[c * n + q];
+                o.lam = A.dpar[0 * n + q];
+                o.mu = A.dpar[1 * n + q];
+                o.b = A.dpar[2 * n + q];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) o.N[c] = A.dpar[(3 + c) * n + q];
+            }
+            inv3(Fc, Ji);
+            s = w * det3(Fc);
+        }
+        if constexpr (kStiff || kForce) {
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                double La[3] = {0.0, 0.0, 0.0};
+                if (active) {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+                        La[k] = sdN[l][a][0] * Ji[0 * 3 + k] + sdN[l][a][1] * Ji[1 * 3 + k] +
+                                sdN[l][a][2] * Ji[2 * 3 + k];
+                }
+                // g_a = s sigma L_a (sigma symmetric: 11 22 33 23 13 12)
+                double g0 = s * (o.sig[0] * La[0] + o.sig[5] * La[1] + o.sig[4] * La[2]);
+                double g1 = s * (o.sig[5] * La[0] + o.sig[1] * La[1] + o.sig[3] * La[2]);
+                double g2 = s * (o.sig[4] * La[0] + o.sig[3] * La[1] + o.sig[2] * La[2]);
+                if (active) {
+                    if constexpr (kStiff) {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) sL[le][l * NPE * 3 + 3 * a + k] = (Real)La[k];
+                    }
+                    if constexpr (kFinite && kStiff) {
+                        sG[le][l * NPE * 3 + 3 * a + 0] = g0;
+                        sG[le][l * NPE * 3 + 3 * a + 1] = g1;
+                        sG[le][l * NPE * 3 + 3 * a + 2] = g2;
+                    }
+                }
+                if constexpr (kForce) {
+                    // sum over the group's points (inactive lanes contribute zero)
+#pragma unroll
+                    for (int off = G / 2; off > 0; off >>= 1) {
+                        g0 += __shfl_xor_sync(0xffffffffu, g0, off);
+                        g1 += __shfl_xor_sync(0xffffffffu, g1, off);
+                        g2 += __shfl_xor_sync(0xffffffffu, g2, off);
+                    }
+                    if (a % G == lane) {
+                        fown[a / G][0] = g0;
+                        fown[a / G][1] = g1;
+                        fown[a / G][2] = g2;
+                    }
+                }
+            }
+            if (active) {
+                if constexpr (kJ2 && kStiff) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) sN[le][l * 6 + c] = (Real)o.N[c];
+                }
+                sC[le][l][0] = (Real)(s * o.lam);
+                sC[le][l][1] = (Real)(s * o.mu);
+                sC[le][l][2] = (Real)(s * o.b);
+                sC[le][l][3] = (Real)0;
+            }
+        }
+    }
+    __syncthreads();
+    if (!valid) return;
+
+    if constexpr (kForce) {
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+            const int a = lane + j * G;
+            if (a < NPE) {
+                atomicAdd(&A.fint[3ll * node[j] + 0], fown[j][0]);
+                atomicAdd(&A.fint[3ll * node[j] + 1], fown[j][1]);
+                atomicAdd(&A.fint[3ll * node[j] + 2], fown[j][2]);
+            }
+        }
+    }
+
+    if constexpr (kStiff) {
+        const int* seg = (NPE == 8) ? c_seg_hex8[lane] : c_seg_tet4[lane];
+        const int r0 = seg[0], b0s = seg[1], n0 = seg[2], r1 = seg[3], b1s = seg[4], n1 = seg[5];
+        const int nb = n0 + n1;
+        const int* slot = A.slot + e * (NPE * NPE);
+        Real* Kp;
+        if constexpr (sizeof(Real) == 8)
+            Kp = reinterpret_cast<Real*>(A.K64);
+        else
+            Kp = reinterpret_cast<Real*>(A.K32);
+        constexpr int PASS = 3;
+#pragma unroll
+        for (int jb = 0; jb < MAXB; jb += PASS) {
+            if (jb >= nb) break;
+            Real acc[PASS][9];
+#pragma unroll
+            for (int j = 0; j < PASS; ++j)
+#pragma unroll
+                for (int i = 0; i < 9; ++i) acc[j][i] = (Real)0;
+            for (int l = 0; l < NQ; ++l) {
+                const Real* Ll = &sL[le][l * NPE * 3];
+                const Real cl = sC[le][l][0], cm = sC[le][l][1], cb = sC[le][l][2];
+                Real Nq[6];
+                if constexpr (kJ2) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) Nq[c] = sN[le][l * 6 + c];
+                }
+                Real Lr0[3], Lr1[3], vr0[3], vr1[3], gr0[3], gr1[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    Lr0[k] = Ll[3 * r0 + k];
+                    Lr1[k] = Ll[3 * r1 + k];
+                    if constexpr (kFinite) {
+                        gr0[k] = (Real)sG[le][l * NPE * 3 + 3 * r0 + k];
+                        gr1[k] = (Real)sG[le][l * NPE * 3 + 3 * r1 + k];
+                    }
+                }
+                if constexpr (kJ2) {
+                    vr0[0] = Nq[0] * Lr0[0] + Nq[5] * Lr0[1] + Nq[4] * Lr0[2];
+                    vr0[1] = Nq[5] * Lr0[0] + Nq[1] * Lr0[1] + Nq[3] * Lr0[2];
+                    vr0[2] = Nq[4] * Lr0[0] + Nq[3] * Lr0[1] + Nq[2] * Lr0[2];
+                    vr1[0] = Nq[0] * Lr1[0] + Nq[5] * Lr1[1] + Nq[4] * Lr1[2];
+                    vr1[1] = Nq[5] * Lr1[0] + Nq[1] * Lr1[1] + Nq[3] * Lr1[2];
+                    vr1[2] = Nq[4] * Lr1[0] + Nq[3] * Lr1[1] + Nq[2] * Lr1[2];
+                }
+#pragma unroll
+                for (int jj = 0; jj < PASS; ++jj) {
+                    const int j = jb + jj;
+                    if (j < nb) {
+                        const bool in0 = j < n0;
+                        const int b = in0 ? b0s + j : b1s + (j - n0);
+                        Real La[3], Lb[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            La[k] = in0 ? Lr0[k] : Lr1[k];
+                            Lb[k] = Ll[3 * b + k];
+                        }
+                        const Real d = La[0] * Lb[0] + La[1] * Lb[1] + La[2] * Lb[2];
+                        Real diag = cm * d;
+                        if constexpr (kFinite) {
+                            diag += (in0 ? gr0[0] : gr1[0]) * Lb[0] +
+                                    (in0 ? gr0[1] : gr1[1]) * Lb[1] +
+                                    (in0 ? gr0[2] : gr1[2]) * Lb[2];
+                        }
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                Real v = cl * La[i] * Lb[k] + cm * La[k] * Lb[i];
+                                if (i == k) v += diag;
+                                acc[jj][3 * i + k] += v;
+                            }
+                        if constexpr (kJ2) {
+                            if (cb != (Real)0) {
+                                Real va[3], vb[3];
+#pragma unroll
+                                for (int k = 0; k < 3; ++k) va[k] = in0 ? vr0[k] : vr1[k];
+                                vb[0] = Nq[0] * Lb[0] + Nq[5] * Lb[1] + Nq[4] * Lb[2];
+                                vb[1] = Nq[5] * Lb[0] + Nq[1] * Lb[1] + Nq[3] * Lb[2];
+                                vb[2] = Nq[4] * Lb[0] + Nq[3] * Lb[1] + Nq[2] * Lb[2];
+#pragma unroll
+                                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                                    for (int k = 0; k < 3; ++k)
+                                        acc[jj][3 * i + k] += cb * va[i] * vb[k];
+                            }
+                        }
+                    }
+                }
+            }
+            // scatter this pass: the block and (off the diagonal) its transpose
+#pragma unroll
+            for (int jj = 0; jj < PASS; ++jj) {
+                const int j = jb + jj;
+                if (j < nb) {
+                    const bool in0 = j < n0;
+                    const int a = in0 ? r0 : r1;
+                    const int b = in0 ? b0s + j : b1s + (j - n0);
+                    const long long sab = slot[a * NPE + b];
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) atomicAdd(&Kp[9 * sab + i], acc[jj][i]);
+                    if (a != b) {
+                        const long long sba = slot[b * NPE + a];
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int k = 0; k < 3; ++k)
+                                atomicAdd(&Kp[9 * sba + 3 * k + i], acc[jj][3 * i + k]);
+                    }
+                }
+            }
+        }
+    }
+}

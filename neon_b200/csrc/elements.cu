@@ -249,39 +249,33 @@ __device__ __forceinline__ void report_status(DeviceStatus* st, int code) {
     atomicOr(&st->flags, 1u << (code - 1));
 }
 
+#include "element_kernel.cuh"
+
 // ---------------------------------------------------------------------------------------
-// The kernel
+// Matrix-free FP64 product y += K v with the tangent of the last stored update: the defect
+// residual of the mixed-precision solve.  With G = sum_b v_b (x) L_b (the gradient of v) the
+// element force of node a is
+//   y_a = s [lam' tr(G) La + mu' (G + G^T) La + b (N:G) N La + G sigma La]
+// -- the same tangent the assembled K holds, applied without forming it.
 // ---------------------------------------------------------------------------------------
-template <int NPE, int MODEL, typename Real, int MODE>
-__global__ void __launch_bounds__(64) k_element(ElementArgs A) {
+template <int NPE, int MODEL>
+__global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __restrict__ v,
+                                              double* __restrict__ y) {
     using T = Topo<NPE>;
-    constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC, MAXB = T::MAXB;
+    constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC;
     constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
     constexpr bool kJ2 = (MODEL == MODEL_J2);
-    constexpr bool kCon = (MODE & MODE_CONSTITUTIVE) != 0;
-    constexpr bool kStiff = (MODE & MODE_STIFFNESS) != 0;
-    constexpr bool kForce = (MODE & MODE_FORCE) != 0;
-    constexpr bool kStore = (MODE & MODE_STORE) != 0;
-    constexpr int NV = kJ2 ? NPE * 3 : 1;
-
-    __shared__ double sX[EPC][NPE][3];
     __shared__ double sx[EPC][NPE][3];
+    __shared__ double sv[EPC][NPE][3];
     __shared__ double sdN[NQ][NPE][3];
-    __shared__ Real sL[EPC][NQ][NPE * 3];
-    __shared__ Real sV[EPC][NQ][NV];
-    __shared__ double sG[EPC][NQ][NPE * 3];
-    __shared__ Real sC[EPC][NQ][4];
-
+    __shared__ double sY[EPC][NQ][NPE * 3];
     const int tid = threadIdx.x;
-    const int le = tid / G;     // element within the CTA
-    const int lane = tid % G;   // lane within the element group
+    const int le = tid / G;
+    const int lane = tid % G;
     const long long e = (long long)blockIdx.x * EPC + le;
     const bool valid = e < A.E;
-
     for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
         (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
-
-    // phase 0: gather nodes
     int node[(NPE + G - 1) / G];
 #pragma unroll
     for (int j = 0; j < (NPE + G - 1) / G; ++j) {
@@ -292,19 +286,17 @@ __global__ void __launch_bounds__(64) k_element(ElementArgs A) {
             node[j] = nd;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                double Xv = A.X[3ll * nd + k];
-                sX[le][a][k] = Xv;
-                sx[le][a][k] = A.u[3ll * nd + k] + Xv;
+                sx[le][a][k] = A.u[3ll * nd + k] + A.X[3ll * nd + k];
+                sv[le][a][k] = v[3ll * nd + k];
             }
         }
     }
     __syncthreads();
-
-    // phase 1: quadrature points
     for (int l = lane; l < NQ; l += G) {
         if (!valid) break;
         const double w = (NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0);
         const long long q = e * NQ + l;
+        const long long n = A.nqp;
         double Fc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int a = 0; a < NPE; ++a)
@@ -312,223 +304,84 @@ __global__ void __launch_bounds__(64) k_element(ElementArgs A) {
             for (int i = 0; i < 3; ++i)
 #pragma unroll
                 for (int k = 0; k < 3; ++k) Fc[i * 3 + k] += sx[le][a][i] * sdN[l][a][k];
-        QpOut o;
-        if constexpr (kCon) {
-            double F0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        double Ji[9];
+        inv3(Fc, Ji);
+        const double s = w * det3(Fc);
+        double L[NPE][3];
+        double Gm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-            for (int a = 0; a < NPE; ++a)
+        for (int a = 0; a < NPE; ++a) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                L[a][k] = sdN[l][a][0] * Ji[0 * 3 + k] + sdN[l][a][1] * Ji[1 * 3 + k] +
+                          sdN[l][a][2] * Ji[2 * 3 + k];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) Gm[i * 3 + k] += sv[le][a][i] * L[a][k];
+        }
+        const double lam = A.dpar[0 * n + q], mu = A.dpar[1 * n + q];
+        const double trG = Gm[0] + Gm[4] + Gm[8];
+        double bN = 0.0, N6[6] = {0, 0, 0, 0, 0, 0};
+        if constexpr (kJ2) {
+            const double b = A.dpar[2 * n + q];
+            if (b != 0.0) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) N6[c] = A.dpar[(3 + c) * n + q];
+                // N:G with N symmetric (11 22 33 23 13 12)
+                bN = b * (N6[0] * Gm[0] + N6[1] * Gm[4] + N6[2] * Gm[8] +
+                          N6[3] * (Gm[5] + Gm[7]) + N6[4] * (Gm[2] + Gm[6]) +
+                          N6[5] * (Gm[1] + Gm[3]));
+            }
+        }
+        double sg[6] = {0, 0, 0, 0, 0, 0};
+        if constexpr (kFinite) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) sg[c] = A.sig[c * n + q];
+        }
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+            const double* La = L[a];
+            double t[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                t[i] = lam * trG * La[i] +
+                       mu * ((Gm[i * 3 + 0] + Gm[0 * 3 + i]) * La[0] +
+                             (Gm[i * 3 + 1] + Gm[1 * 3 + i]) * La[1] +
+                             (Gm[i * 3 + 2] + Gm[2 * 3 + i]) * La[2]);
+            if constexpr (kJ2) {
+                t[0] += bN * (N6[0] * La[0] + N6[5] * La[1] + N6[4] * La[2]);
+                t[1] += bN * (N6[5] * La[0] + N6[1] * La[1] + N6[3] * La[2]);
+                t[2] += bN * (N6[4] * La[0] + N6[3] * La[1] + N6[2] * La[2]);
+            }
+            if constexpr (kFinite) {
+                const double sl0 = sg[0] * La[0] + sg[5] * La[1] + sg[4] * La[2];
+                const double sl1 = sg[5] * La[0] + sg[1] * La[1] + sg[3] * La[2];
+                const double sl2 = sg[4] * La[0] + sg[3] * La[1] + sg[2] * La[2];
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) F0[i * 3 + k] += sX[le][a][i] * sdN[l][a][k];
-            double F0i[9];
-            inv3(F0, F0i);
-            double Hm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-            for (int a = 0; a < NPE; ++a) {
-                double b0[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    b0[k] = sdN[l][a][0] * F0i[0 * 3 + k] + sdN[l][a][1] * F0i[1 * 3 + k] +
-                            sdN[l][a][2] * F0i[2 * 3 + k];
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    double d = sx[le][a][i] - sX[le][a][i];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) Hm[i * 3 + k] += d * b0[k];
-                }
+                    t[i] += Gm[i * 3 + 0] * sl0 + Gm[i * 3 + 1] * sl1 + Gm[i * 3 + 2] * sl2;
             }
-            double Fd[9];
-            matmul3(Fc, F0i, Fd);
-            const double detF = det3(Fd);
-            if (signbit(detF)) {
-                unsigned long long key = ((unsigned long long)q << 32) |
-                                         (unsigned long long)__float_as_uint((float)detF);
-                atomicMin(&A.status->negdet_first, key);
-                atomicAdd(&A.status->negdet_count, 1u);
-                report_status(A.status, NB2_E_NEG_DETJ);
-            }
-            if constexpr (MODEL == MODEL_LE) {
-                cm_linear_elastic(A, Hm, o);
-            } else if constexpr (MODEL == MODEL_NH) {
-                cm_neo_hooke(A, Fd, detF, o);
-            } else if constexpr (MODEL == MODEL_J2) {
-                if (!cm_j2(A, q, Hm, o)) report_status(A.status, NB2_E_RETURN_MAP);
-            } else {
-                cm_microsphere(A, A.Ge ? A.Ge[e] : A.G, Fd, detF, o);
-            }
-            bool bad = isnan(o.lam) || isnan(o.mu);
 #pragma unroll
-            for (int c = 0; c < 6; ++c) bad |= isnan(o.sig[c]);
-            if (bad) report_status(A.status, NB2_E_NAN);
-            if constexpr (kStore) {
-                const long long n = A.nqp;
-#pragma unroll
-                for (int c = 0; c < 6; ++c) A.sig[c * n + q] = o.sig[c];
-                A.dpar[0 * n + q] = o.lam;
-                A.dpar[1 * n + q] = o.mu;
-                A.dpar[2 * n + q] = o.b;
-#pragma unroll
-                for (int c = 0; c < 6; ++c) A.dpar[(3 + c) * n + q] = kJ2 ? o.N[c] : 0.0;
-                A.detF[q] = detF;
-            }
-        } else {
-            const long long n = A.nqp;
-#pragma unroll
-            for (int c = 0; c < 6; ++c) o.sig[c] = A.sig[c * n + q];
-            o.lam = A.dpar[0 * n + q];
-            o.mu = A.dpar[1 * n + q];
-            o.b = A.dpar[2 * n + q];
-#pragma unroll
-            for (int c = 0; c < 6; ++c) o.N[c] = A.dpar[(3 + c) * n + q];
-        }
-        if constexpr (kStiff || kForce) {
-            double Ji[9];
-            inv3(Fc, Ji);
-            const double s = w * det3(Fc);
-#pragma unroll
-            for (int a = 0; a < NPE; ++a) {
-                double La[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    La[k] = sdN[l][a][0] * Ji[0 * 3 + k] + sdN[l][a][1] * Ji[1 * 3 + k] +
-                            sdN[l][a][2] * Ji[2 * 3 + k];
-                // g_a = s sigma L_a  (sigma symmetric: 11 22 33 23 13 12)
-                sG[le][l][3 * a + 0] = s * (o.sig[0] * La[0] + o.sig[5] * La[1] + o.sig[4] * La[2]);
-                sG[le][l][3 * a + 1] = s * (o.sig[5] * La[0] + o.sig[1] * La[1] + o.sig[3] * La[2]);
-                sG[le][l][3 * a + 2] = s * (o.sig[4] * La[0] + o.sig[3] * La[1] + o.sig[2] * La[2]);
-                if constexpr (kStiff) {
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) sL[le][l][3 * a + k] = (Real)La[k];
-                    if constexpr (kJ2) {
-                        sV[le][l][3 * a + 0] = (Real)(o.N[0] * La[0] + o.N[5] * La[1] + o.N[4] * La[2]);
-                        sV[le][l][3 * a + 1] = (Real)(o.N[5] * La[0] + o.N[1] * La[1] + o.N[3] * La[2]);
-                        sV[le][l][3 * a + 2] = (Real)(o.N[4] * La[0] + o.N[3] * La[1] + o.N[2] * La[2]);
-                    }
-                }
-            }
-            sC[le][l][0] = (Real)(s * o.lam);
-            sC[le][l][1] = (Real)(s * o.mu);
-            sC[le][l][2] = (Real)(s * o.b);
-            sC[le][l][3] = (Real)0;
+            for (int i = 0; i < 3; ++i) sY[le][l][3 * a + i] = s * t[i];
         }
     }
     __syncthreads();
     if (!valid) return;
-
-    if constexpr (kForce) {
-        // internal force of node a: sum_q g_a(q)
 #pragma unroll
-        for (int j = 0; j < (NPE + G - 1) / G; ++j) {
-            int a = lane + j * G;
-            if (a < NPE) {
-                double f0 = 0, f1 = 0, f2 = 0;
+    for (int j = 0; j < (NPE + G - 1) / G; ++j) {
+        int a = lane + j * G;
+        if (a < NPE) {
+            double f0 = 0, f1 = 0, f2 = 0;
 #pragma unroll
-                for (int l = 0; l < NQ; ++l) {
-                    f0 += sG[le][l][3 * a + 0];
-                    f1 += sG[le][l][3 * a + 1];
-                    f2 += sG[le][l][3 * a + 2];
-                }
-                atomicAdd(&A.fint[3ll * node[j] + 0], f0);
-                atomicAdd(&A.fint[3ll * node[j] + 1], f1);
-                atomicAdd(&A.fint[3ll * node[j] + 2], f2);
+            for (int l = 0; l < NQ; ++l) {
+                f0 += sY[le][l][3 * a + 0];
+                f1 += sY[le][l][3 * a + 1];
+                f2 += sY[le][l][3 * a + 2];
             }
-        }
-    }
-
-    if constexpr (kStiff) {
-        const int* seg = (NPE == 8) ? c_seg_hex8[lane] : c_seg_tet4[lane];
-        const int r0 = seg[0], b0s = seg[1], n0 = seg[2], r1 = seg[3], b1s = seg[4], n1 = seg[5];
-        Real acc[MAXB][9];
-#pragma unroll
-        for (int j = 0; j < MAXB; ++j)
-#pragma unroll
-            for (int i = 0; i < 9; ++i) acc[j][i] = (Real)0;
-
-        for (int l = 0; l < NQ; ++l) {
-            const Real cl = sC[le][l][0], cm = sC[le][l][1], cb = sC[le][l][2];
-            Real L0[3], L1[3], g0[3], g1[3], v0[3], v1[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                L0[k] = sL[le][l][3 * r0 + k];
-                L1[k] = sL[le][l][3 * r1 + k];
-                if constexpr (kFinite) {
-                    g0[k] = (Real)sG[le][l][3 * r0 + k];
-                    g1[k] = (Real)sG[le][l][3 * r1 + k];
-                }
-                if constexpr (kJ2) {
-                    v0[k] = sV[le][l][3 * r0 + k];
-                    v1[k] = sV[le][l][3 * r1 + k];
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < MAXB; ++j) {
-                const bool in0 = j < n0;
-                if (j < n0 + n1) {
-                    const int b = in0 ? b0s + j : b1s + (j - n0);
-                    Real La[3], Lb[3];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        La[k] = in0 ? L0[k] : L1[k];
-                        Lb[k] = sL[le][l][3 * b + k];
-                    }
-                    Real d = La[0] * Lb[0] + La[1] * Lb[1] + La[2] * Lb[2];
-                    Real diag = cm * d;
-                    if constexpr (kFinite) {
-                        diag += (in0 ? g0[0] : g1[0]) * Lb[0] + (in0 ? g0[1] : g1[1]) * Lb[1] +
-                                (in0 ? g0[2] : g1[2]) * Lb[2];
-                    }
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            Real v = cl * La[i] * Lb[k] + cm * La[k] * Lb[i];
-                            if (i == k) v += diag;
-                            acc[j][3 * i + k] += v;
-                        }
-                    if constexpr (kJ2) {
-                        if (cb != (Real)0) {
-                            Real va[3], vb[3];
-#pragma unroll
-                            for (int k = 0; k < 3; ++k) {
-                                va[k] = in0 ? v0[k] : v1[k];
-                                vb[k] = sV[le][l][3 * b + k];
-                            }
-#pragma unroll
-                            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                                for (int k = 0; k < 3; ++k) acc[j][3 * i + k] += cb * va[i] * vb[k];
-                        }
-                    }
-                }
-            }
-        }
-
-        // phase 3: scatter (red.global.add) of the upper blocks and their transposes
-        const int* slot = A.slot + e * (NPE * NPE);
-#pragma unroll
-        for (int j = 0; j < MAXB; ++j) {
-            if (j < n0 + n1) {
-                const bool in0 = j < n0;
-                const int a = in0 ? r0 : r1;
-                const int b = in0 ? b0s + j : b1s + (j - n0);
-                const long long sab = slot[a * NPE + b];
-                Real* Kp = nullptr;
-                if constexpr (sizeof(Real) == 8)
-                    Kp = reinterpret_cast<Real*>(A.K64);
-                else
-                    Kp = reinterpret_cast<Real*>(A.K32);
-#pragma unroll
-                for (int i = 0; i < 9; ++i) atomicAdd(&Kp[9 * sab + i], acc[j][i]);
-                if (a != b) {
-                    const long long sba = slot[b * NPE + a];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int k = 0; k < 3; ++k)
-                            atomicAdd(&Kp[9 * sba + 3 * k + i], acc[j][3 * i + k]);
-                }
-            }
+            atomicAdd(&y[3ll * node[j] + 0], f0);
+            atomicAdd(&y[3ll * node[j] + 1], f1);
+            atomicAdd(&y[3ll * node[j] + 2], f2);
         }
     }
 }
@@ -592,8 +445,12 @@ static int dispatch_mode(nb2_ctx* c, const ElementArgs& A, int mode, int precisi
     constexpr int RESID = MODE_CONSTITUTIVE | MODE_FORCE;
     constexpr int UPD = MODE_CONSTITUTIVE | MODE_STORE;
     constexpr int ASM = MODE_STIFFNESS | MODE_FORCE;
+    constexpr int FUSED_STORE = FUSED | MODE_STORE;
     if (mode == FUSED && precision == NB2_FP64) launch_one<NPE, MODEL, double, FUSED>(c, A);
     else if (mode == FUSED) launch_one<NPE, MODEL, float, FUSED>(c, A);
+    else if (mode == FUSED_STORE && precision != NB2_FP64)
+        launch_one<NPE, MODEL, float, FUSED_STORE>(c, A);
+    else if (mode == (RESID | MODE_STORE)) launch_one<NPE, MODEL, double, RESID | MODE_STORE>(c, A);
     else if (mode == RESID) launch_one<NPE, MODEL, double, RESID>(c, A);
     else if (mode == UPD) launch_one<NPE, MODEL, double, UPD>(c, A);
     else if (mode == ASM) launch_one<NPE, MODEL, double, ASM>(c, A);
@@ -610,6 +467,62 @@ static int dispatch_model(nb2_ctx* c, const ElementArgs& A, int mode, int precis
         case MODEL_MS: return dispatch_mode<NPE, MODEL_MS>(c, A, mode, precision);
     }
     return NB2_E_INPUT;
+}
+
+static ElementArgs make_args(nb2_ctx* c);
+
+template <int NPE>
+static void launch_apply_t(nb2_ctx* c, const ElementArgs& A, const double* v, double* y) {
+    constexpr int EPC = Topo<NPE>::EPC, G = Topo<NPE>::G;
+    unsigned grid = (unsigned)((c->E + EPC - 1) / EPC);
+    switch (c->mat.model) {
+        case MODEL_LE: k_apply<NPE, MODEL_LE><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+        case MODEL_NH: k_apply<NPE, MODEL_NH><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+        case MODEL_J2: k_apply<NPE, MODEL_J2><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+        default: k_apply<NPE, MODEL_MS><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+    }
+    c->launches++;
+}
+
+// y = K v (FP64, matrix-free) with the tangent stored by the last MODE_STORE pass
+int launch_apply(nb2_ctx* c, const double* v, double* y) {
+    int st = upload_tables(c);
+    if (st) return st;
+    if (!c->dpar) return NB2_E_INPUT;
+    ElementArgs A = make_args(c);
+    NB2_CUDA(c, cudaMemsetAsync(y, 0, sizeof(double) * c->n, c->stream));
+    if (c->npe == 8)
+        launch_apply_t<8>(c, A, v, y);
+    else
+        launch_apply_t<4>(c, A, v, y);
+    NB2_CUDA(c, cudaGetLastError());
+    return NB2_OK;
+}
+
+static ElementArgs make_args(nb2_ctx* c) {
+    ElementArgs A;
+    A.X = c->X;
+    A.u = c->u;
+    A.conn = c->conn;
+    A.slot = c->slot;
+    A.E = c->E;
+    A.nqp = c->nqp;
+    A.K = c->mat.bulk_modulus;
+    A.G = c->mat.shear_modulus;
+    A.lambda = c->mat.bulk_modulus - 2.0 * c->mat.shear_modulus / 3.0;
+    A.sigma_y = c->mat.yield_stress;
+    A.H_iso = c->mat.isotropic_hardening_modulus;
+    A.Ge = c->Ge;
+    A.ep = c->ep;
+    A.epbar = c->epbar;
+    A.K64 = c->K64;
+    A.K32 = c->K32;
+    A.fint = c->fint;
+    A.sig = c->sig;
+    A.dpar = c->dpar;
+    A.detF = c->detF;
+    A.status = c->status;
+    return A;
 }
 
 int launch_element_kernel(nb2_ctx* c, int mode, int precision) {

@@ -116,21 +116,45 @@ struct Csr {
     int rows;
 };
 
-// y[3a+r] for r = 0..2 of block row a, reduced across the warp; returned in lane 0.
+// y[3a+r] for r = 0..2 of block row a, reduced across the warp (all lanes get the sums).
+// A row of a hex8 mesh holds up to 27 blocks = 243 values: the first 256 values are loaded in one
+// batch of 8 independent loads per lane (values, then their block columns, then the x entries),
+// so a warp keeps a whole row in flight instead of one 32-value slice per round trip.
 template <typename V, typename X, typename Acc>
 __device__ __forceinline__ void bsr_row(const Bsr<V>& A, const X* __restrict__ x, int a, int lane,
                                         Acc& y0, Acc& y1, Acc& y2) {
-    const int b0 = A.brp[a];
-    const int deg = A.brp[a + 1] - b0;
+    const int b0 = __ldg(A.brp + a);
+    const int nval = 9 * (__ldg(A.brp + a + 1) - b0);
     const V* vals = A.val + 9ll * b0;
     const int* cols = A.bcol + b0;
     Acc a0 = 0, a1 = 0, a2 = 0;
-    for (int v = lane; v < 9 * deg; v += 32) {
-        const int k = v / 9;
-        const int e = v - 9 * k;
+    constexpr int U = 8;
+    V v[U];
+    int c[U];
+#pragma unroll
+    for (int t = 0; t < U; ++t) {
+        const int idx = lane + 32 * t;
+        const bool ok = idx < nval;
+        v[t] = ok ? ld_stream(vals + idx) : (V)0;
+        c[t] = ok ? __ldg(cols + idx / 9) : 0;
+    }
+#pragma unroll
+    for (int t = 0; t < U; ++t) {
+        const int idx = lane + 32 * t;
+        const int e = idx % 9;
         const int r = e / 3;
         const int cc = e - 3 * r;
-        const Acc prod = (Acc)ld_stream(vals + v) * (Acc)x[3ll * __ldg(cols + k) + cc];
+        const Acc prod = (Acc)v[t] * (Acc)x[3ll * c[t] + cc];
+        a0 += (r == 0) ? prod : (Acc)0;
+        a1 += (r == 1) ? prod : (Acc)0;
+        a2 += (r == 2) ? prod : (Acc)0;
+    }
+    for (int idx = lane + 32 * U; idx < nval; idx += 32) {  // rows with more than 28 blocks
+        const int k = idx / 9;
+        const int e = idx - 9 * k;
+        const int r = e / 3;
+        const int cc = e - 3 * r;
+        const Acc prod = (Acc)ld_stream(vals + idx) * (Acc)x[3ll * __ldg(cols + k) + cc];
         a0 += (r == 0) ? prod : (Acc)0;
         a1 += (r == 1) ? prod : (Acc)0;
         a2 += (r == 2) ? prod : (Acc)0;
@@ -169,8 +193,193 @@ __global__ void __launch_bounds__(kRedThreads) k_spmv(Bsr<V> A, const X* __restr
         if (threadIdx.x == 0) {
             s->pq = tot[0];
             s->alpha = s->abs_new / tot[0];
-            if (!(tot[0] > 0.0) || !isfinite(s->alpha)) {
-                s->status = NB2_E_CG_BREAKDOWN;
+            // Eigen's CG carries on through p.Ap <= 0 (an indefinite tangent); only a
+            // non-finite step size is a failure (neon: FE_INVALID -> computational_error)
+            if (!isfinite(s->alpha)) {
+                s->status = NB2_E_NAN;
+                s->done = 1;
+            }
+            s->counter[0] = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Bulk-copy pipelined SpMV (sm_100a).  A block row's values ([deg][9]) and block columns are
+// contiguous, and so is a chunk of R consecutive block rows.  One elected thread streams the
+// chunks a CTA owns into a ring of shared-memory stages with cp.async.bulk (completion on an
+// mbarrier, L2 evict-first so the gathered vector stays resident), while the 8 warps compute on
+// the stage that has landed: lane = block of the row, 9 values from shared memory, the 3 x
+// entries of the block column from L2, 3 partial row sums reduced across the warp.  Every wait
+// on an mbarrier is bounded: on expiry the kernel records NB2_E_TIMEOUT and stops issuing.
+// ---------------------------------------------------------------------------------------
+constexpr int kStages = 3;
+constexpr unsigned kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    for (unsigned i = 0; i < kWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          unsigned long long* bar, unsigned long long policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
+        "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+struct BulkPlan {
+    int rows_per_chunk;
+    int chunks;
+    int stage_val_bytes;  // per stage, 16-byte multiple
+    int stage_col_bytes;
+};
+
+// byte range [lo, hi) of elements [b0, b1) of an array of `size`-byte items, widened to 16 B
+__device__ __forceinline__ void span16(long long b0, long long b1, int size, long long& lo,
+                                       long long& hi) {
+    lo = (b0 * size) & ~15ll;
+    hi = (b1 * size + 15) & ~15ll;
+}
+
+template <typename V, typename X>
+__global__ void __launch_bounds__(kRedThreads) k_spmv_bulk(Bsr<V> A, BulkPlan plan,
+                                                           const X* __restrict__ p,
+                                                           X* __restrict__ q,
+                                                           const unsigned char* __restrict__ mask,
+                                                           CgScalars* s, double* partials) {
+    if (s->done) return;
+    extern __shared__ __align__(128) unsigned char dyn[];
+    __shared__ unsigned long long bar[kStages];
+    __shared__ int timed_out;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    unsigned char* stage_base[kStages];
+#pragma unroll
+    for (int i = 0; i < kStages; ++i)
+        stage_base[i] = dyn + i * (plan.stage_val_bytes + plan.stage_col_bytes);
+    unsigned long long policy = 0;
+    if (tid == 0) {
+        for (int i = 0; i < kStages; ++i) mbar_init(&bar[i], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
+        timed_out = 0;
+    }
+    __syncthreads();
+    // chunks of this CTA: blockIdx.x, blockIdx.x + gridDim.x, ...
+    const int my_chunks = (plan.chunks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    auto issue = [&](int j) {  // thread 0 only
+        const int c = blockIdx.x + j * gridDim.x;
+        const int r0 = c * plan.rows_per_chunk;
+        const int r1 = min(r0 + plan.rows_per_chunk, A.rows);
+        const long long b0 = A.brp[r0], b1 = A.brp[r1];
+        long long vlo, vhi, clo, chi;
+        span16(9 * b0, 9 * b1, (int)sizeof(V), vlo, vhi);
+        span16(b0, b1, 4, clo, chi);
+        const int st = j % kStages;
+        unsigned char* dst = stage_base[st];
+        mbar_expect_tx(&bar[st], (unsigned)((vhi - vlo) + (chi - clo)));
+        bulk_load(dst, reinterpret_cast<const unsigned char*>(A.val) + vlo, (unsigned)(vhi - vlo),
+                  &bar[st], policy);
+        bulk_load(dst + plan.stage_val_bytes, reinterpret_cast<const unsigned char*>(A.bcol) + clo,
+                  (unsigned)(chi - clo), &bar[st], policy);
+    };
+    int last_issued = -1;  // thread 0 only
+    if (tid == 0)
+        for (int j = 0; j < kStages - 1 && j < my_chunks; ++j) {
+            issue(j);
+            last_issued = j;
+        }
+    double dot[1] = {0.0};
+    int consumed = -1;
+    for (int j = 0; j < my_chunks; ++j) {
+        const int st = j % kStages;
+        const bool stop = timed_out != 0;  // stable: written only before a __syncthreads
+        if (tid == 0 && j + kStages - 1 < my_chunks && !stop) {
+            // the stage being refilled was read in iteration j-1 (all threads passed the
+            // barrier below); order those generic reads before the async-proxy writes
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(j + kStages - 1);
+            last_issued = j + kStages - 1;
+        }
+        const unsigned parity = (unsigned)((j / kStages) & 1);
+        if (!stop && !mbar_wait(&bar[st], parity)) atomicExch(&timed_out, 1);
+        __syncthreads();
+        if (!timed_out) {
+            consumed = j;
+            const int c = blockIdx.x + j * gridDim.x;
+            const int r0 = c * plan.rows_per_chunk;
+            const int r1 = min(r0 + plan.rows_per_chunk, A.rows);
+            const long long cb0 = A.brp[r0];
+            const long long voff = (9 * cb0 * (long long)sizeof(V)) & 15ll;  // bytes
+            const long long coff = (cb0 * 4) & 15ll;
+            const V* sv = reinterpret_cast<const V*>(stage_base[st] + voff);
+            const int* sc = reinterpret_cast<const int*>(stage_base[st] + plan.stage_val_bytes + coff);
+            for (int row = r0 + warp; row < r1; row += nwarps) {
+                const int rb = A.brp[row] - (int)cb0;
+                const int deg = A.brp[row + 1] - A.brp[row];
+                X a0 = 0, a1 = 0, a2 = 0;
+                for (int k = lane; k < deg; k += 32) {
+                    const int col = sc[rb + k];
+                    const X x0 = __ldg(p + 3ll * col), x1 = __ldg(p + 3ll * col + 1),
+                            x2 = __ldg(p + 3ll * col + 2);
+                    const V* blk = sv + 9 * (rb + k);
+                    a0 += (X)blk[0] * x0 + (X)blk[1] * x1 + (X)blk[2] * x2;
+                    a1 += (X)blk[3] * x0 + (X)blk[4] * x1 + (X)blk[5] * x2;
+                    a2 += (X)blk[6] * x0 + (X)blk[7] * x1 + (X)blk[8] * x2;
+                }
+                a0 = warp_sum(a0);
+                a1 = warp_sum(a1);
+                a2 = warp_sum(a2);
+                if (lane < 3) {
+                    const long long i = 3ll * row + lane;
+                    X y = lane == 0 ? a0 : (lane == 1 ? a1 : a2);
+                    if (mask && mask[i]) y = (X)0;
+                    q[i] = y;
+                    dot[0] += (double)p[i] * (double)y;
+                }
+            }
+        }
+        __syncthreads();  // stage st is free for the producer
+    }
+    if (timed_out && tid == 0) {
+        // let the copies still in flight land before the CTA exits (bounded waits)
+        for (int j = consumed + 1; j <= last_issued; ++j)
+            mbar_wait(&bar[j % kStages], (unsigned)((j / kStages) & 1));
+        s->status = NB2_E_TIMEOUT;
+        s->done = 1;
+    }
+    if (block_partials<1>(dot, partials, &s->counter[0])) {
+        double tot[1];
+        final_sum<1>(partials, tot);
+        if (threadIdx.x == 0) {
+            s->pq = tot[0];
+            s->alpha = s->abs_new / tot[0];
+            if (!isfinite(s->alpha)) {
+                s->status = NB2_E_NAN;
                 s->done = 1;
             }
             s->counter[0] = 0;
@@ -404,6 +613,30 @@ static int wait_scalars(nb2_ctx* c) {
 }
 
 constexpr int kChunk = 32;
+constexpr int kBulkSmemBudget = 110 * 1024;  // per CTA: two CTAs per SM
+constexpr int kBulkCtasPerSm = 2;
+
+// Rows per chunk and stage sizes of the bulk SpMV: the largest power-of-two chunk whose
+// kStages stages fit the shared-memory budget (spans widened to 16 B as the copies are).
+static bool make_bulk_plan(const nb2_ctx* c, int vsize, BulkPlan* plan) {
+    for (int R = 64; R >= 2; R /= 2) {
+        long long maxv = 0, maxc = 0;
+        const int chunks = (c->N + R - 1) / R;
+        for (int ch = 0; ch < chunks; ++ch) {
+            const long long b0 = c->h_brp[(size_t)ch * R];
+            const long long b1 = c->h_brp[std::min((size_t)(ch + 1) * R, (size_t)c->N)];
+            const long long vlo = (9 * b0 * vsize) & ~15ll, vhi = (9 * b1 * vsize + 15) & ~15ll;
+            const long long clo = (b0 * 4) & ~15ll, chi = (b1 * 4 + 15) & ~15ll;
+            maxv = std::max(maxv, vhi - vlo);
+            maxc = std::max(maxc, chi - clo);
+        }
+        if (kStages * (maxv + maxc) <= kBulkSmemBudget) {
+            *plan = BulkPlan{R, chunks, (int)maxv, (int)maxc};
+            return true;
+        }
+    }
+    return false;
+}
 
 template <typename V, typename X>
 static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv, const double* b,
@@ -411,6 +644,17 @@ static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv,
                       double* error, bool use_graphs, cudaGraphExec_t* cache) {
     const int RB = reduction_blocks(c);
     Bsr<V> A{c->brp, c->bcol, vals, c->N};
+    BulkPlan plan{};
+    const bool bulk = make_bulk_plan(c, (int)sizeof(V), &plan);
+    int bulk_grid = 0;
+    size_t bulk_smem = 0;
+    if (bulk) {
+        bulk_smem = (size_t)kStages * (plan.stage_val_bytes + plan.stage_col_bytes);
+        NB2_CUDA(c, cudaFuncSetAttribute(k_spmv_bulk<V, X>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bulk_smem));
+        bulk_grid = std::min(plan.chunks, 148 * kBulkCtasPerSm);
+    }
     const long long n = c->n;
     k_invdiag<V, X><<<(c->N + 255) / 256, 256, 0, c->stream>>>(A, inv);
     k_init<X><<<RB, kRedThreads, 0, c->stream>>>(n, b, x, r, p, inv, c->cgs, c->partials, tol);
@@ -421,7 +665,12 @@ static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv,
     const unsigned char* mask = use_mask ? c->mask : nullptr;
     auto enqueue = [&](int count) {
         for (int it = 0; it < count; ++it) {
-            k_spmv<V, X><<<RB, kRedThreads, 0, c->stream>>>(A, p, q, mask, c->cgs, c->partials);
+            if (bulk)
+                k_spmv_bulk<V, X><<<bulk_grid, kRedThreads, bulk_smem, c->stream>>>(
+                    A, plan, p, q, mask, c->cgs, c->partials);
+            else
+                k_spmv<V, X><<<RB, kRedThreads, 0, c->stream>>>(A, p, q, mask, c->cgs,
+                                                                c->partials);
             k_xr<X><<<RB, kRedThreads, 0, c->stream>>>(n, x, r, p, q, inv, c->cgs, c->partials);
             k_p<X><<<RB, kRedThreads, 0, c->stream>>>(n, p, r, inv, c->cgs);
         }
@@ -495,6 +744,32 @@ void bsr_spmv_mixed_accum(nb2_ctx* c, const double* x, double* y) {
     Bsr<float> A{c->brp, c->bcol, c->K32, c->N};
     k_bsr_apply<float><<<reduction_blocks(c), kRedThreads, 0, c->stream>>>(A, x, y, nullptr);
     c->launches++;
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_dot1(long long n, const double* a, const double* b,
+                                                      double* partials, unsigned int* counter,
+                                                      double* out) {
+    double acc[1] = {0.0};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        acc[0] += a[i] * b[i];
+    if (block_partials<1>(acc, partials, counter)) {
+        double tot[1];
+        final_sum<1>(partials, tot);
+        if (threadIdx.x == 0) {
+            *out = tot[0];
+            *counter = 0;
+        }
+    }
+}
+
+double device_dot_sync(nb2_ctx* c, const double* a, const double* b, int n) {
+    k_dot1<<<reduction_blocks(c), kRedThreads, 0, c->stream>>>(n, a, b, c->partials,
+                                                                &c->cgs->counter[3], c->norms + 5);
+    c->launches++;
+    cudaMemcpyAsync(c->h_norms + 5, c->norms + 5, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    cudaStreamSynchronize(c->stream);
+    return c->h_norms[5];
 }
 
 int compute_norms(nb2_ctx* c) {

@@ -206,10 +206,15 @@ def config_c2(n: int = 64, seed: int = 20240601, increments: int = 10) -> Proble
     return Problem("c2_neohooke_hex8_%d" % n, mesh, mat, dirichlet_boundaries(mesh, bcs), opts)
 
 
-def config_c3(n: int = 100, steps: int = 20) -> Problem:
+def config_c3(n: int = 100, steps: int = 20, increments_per_step: int = 4) -> Problem:
     """Small-strain J2 plasticity with linear isotropic hardening (E=200e3, nu=0.3, sigma_y=200,
-    H=1e3), n^3 hex8, bottom clamped, top uz = 5e-3 sin(2 pi t / steps) sampled at every unit of
-    time (one cycle, +-5e-3) -- neon's sinusoidal generator with period = steps."""
+    H=1e3), n^3 hex8, bottom clamped, top uz = 5e-3 sin(2 pi t / steps): one +-5e-3 cycle over
+    `steps` time units (neon's sinusoidal generator, period = steps), each unit split into
+    `increments_per_step` load increments (generate_time_step = 1 / increments_per_step).
+
+    With neon's J2 update (plastic strain accumulated at every Newton iteration,
+    small_strain_J2_plasticity.cpp:35-86) full Newton diverges on 1.56e-3 increments of the top
+    displacement once the mesh is 40^3 or finer; 4 increments per unit converge."""
     mesh = structured_hex8(n)
     mat = make_material({"elastic_modulus": 200e3, "poissons_ratio": 0.3, "yield_stress": 200.0,
                          "isotropic_hardening_modulus": 1e3},
@@ -218,10 +223,11 @@ def config_c3(n: int = 100, steps: int = 20) -> Problem:
             "z": [0.0, 0.0]},
            {"name": "top", "generate_type": "sinusoidal", "z": [5e-3], "period": [float(steps)],
             "phase": [0.0], "number_of_cycles": [1.0]}]
+    dt = 1.0 / increments_per_step
     opts = Options(residual_tolerance=1e-8, displacement_tolerance=1e-8, linear_iterations=15,
-                   period=float(steps), initial=1.0, minimum=1.0, maximum=1.0, adaptive=False,
+                   period=float(steps), initial=dt, minimum=dt, maximum=dt, adaptive=False,
                    cg_tolerance=1e-10, cg_maximum_iterations=200000)
-    return Problem("c3_j2_hex8_%d" % n, mesh, mat, dirichlet_boundaries(mesh, bcs, 1.0), opts)
+    return Problem("c3_j2_hex8_%d" % n, mesh, mat, dirichlet_boundaries(mesh, bcs, dt), opts)
 
 
 def config_c4(n: int = 48, seed_field: int = 7, traction: float = 0.05) -> Problem:

@@ -195,15 +195,18 @@ def test_static_solve_parity(api, oracle, name, make):
     assert rel_err(u, u_o) < 1e-10
     # same Newton trajectory: iteration numbers and the norms the convergence test reads
     assert np.array_equal(sm.log[:, :2], log_o[:, :2])
-    big = log_o[:, 3:] > 1e-6
-    np.testing.assert_allclose(sm.log[:, 3:][big], log_o[:, 3:][big], rtol=1e-6)
+    # norms near the CG noise floor (rtol 1e-10 of the step's first residual) differ by CG
+    # round-off; the rest agree to 1e-6
+    for col in (3, 4):
+        floor = 1e-8 * np.abs(log_o[:, col]).max()
+        np.testing.assert_allclose(sm.log[:, col], log_o[:, col], rtol=1e-6, atol=floor)
 
 
 def test_mixed_precision_matches_fp64_device(api):
     pr = P.config_c3(6, steps=20)
     pr.options.period = 5.0  # first five increments of the cycle (into the plastic range)
     u64 = api.StaticMatrix(pr).solve()
-    sm = api.StaticMatrix(pr, precision=api.MIXED, mixed_inner_tolerance=1e-5)
+    sm = api.StaticMatrix(pr, precision=api.MIXED, mixed_inner_tolerance=1e-4)
     u32 = sm.solve()
     assert rel_err(u32, u64) < 1e-8
 
@@ -252,3 +255,20 @@ def test_full_size_c3_assembly_properties(api):
         t = np.zeros(g.ndofs)
         t[k::3] = 1.0
         assert np.abs(A @ t).max() <= 1e-9 * abs(K).max()
+
+
+def test_cpp_adapter_driver(api, oracle):
+    """The C++ adapter (include/neon_b200.hpp) used from a C++ program, as neon would."""
+    import json
+    import subprocess
+    from neon_b200 import build
+    exe = build.build_adapter_driver()
+    out = json.loads(subprocess.run([exe, "4"], check=True, capture_output=True,
+                                    text=True).stdout)
+    np.testing.assert_allclose(out["cg_x"], [1.375, 1.75, 1.625], atol=1e-5)
+    assert out["maxit_threw"] is True
+    pr = P.config_c1(4)
+    rep, u_o, _, _, _ = oracle.static_solve(pr)
+    assert rep["status"] == 0
+    assert out["newton_iterations"] == rep["newton_iterations"]
+    assert rel_err(np.array(out["u"]), u_o) < 1e-10
