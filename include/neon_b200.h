@@ -171,6 +171,11 @@ int nb2_update_internal_variables(nb2_ctx* ctx, const double* u, double time_ste
  * Either pointer may be NULL. */
 int nb2_assemble(nb2_ctx* ctx, double* K_values, double* f_int);
 
+/* Matrix-free tangent product y = K v (host buffers, FP64) with the tangent of the last
+ * nb2_update_internal_variables -- the same K nb2_assemble returns, applied element by element
+ * without forming it (the defect residual of the mixed-precision solve). */
+int nb2_apply_tangent(nb2_ctx* ctx, const double* v, double* y);
+
 /* submesh::save_internal_variables (submesh.cpp:54-64): commit (1) or revert (0). */
 int nb2_save_internal_variables(nb2_ctx* ctx, int32_t converged);
 
@@ -207,6 +212,21 @@ int nb2_static_solve(nb2_ctx* ctx, const nb2_solver_options* options,
                      const nb2_dof_table* dirichlet, int32_t num_dirichlet,
                      const nb2_dof_table* nodal_forces, int32_t num_nodal_forces, double* u_out,
                      nb2_solve_report* report, nb2_newton_log* log, int32_t max_log);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Adjoint                                                                                  */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Gradient of an objective J(u) with respect to the per-element shear modulus of the Gaussian
+ * affine microsphere model (gaussian_affine_microsphere.cpp:23-88), at the equilibrium left by
+ * the last nb2_static_solve on this context (its displacement and Dirichlet set).  dJdu: host
+ * [num_dofs]; dJdG: host [num_elements].  Solves K lambda = dJ/du (K symmetric; precision
+ * NB2_FP64 or NB2_MIXED, relative tolerance `tolerance`) and evaluates
+ * dJ/dG_e = -lambda^T df_int/dG_e element by element, recomputing the quadrature-point state.
+ * Extends the reference (neon has no sensitivities) for its material parameter G. */
+int nb2_adjoint_shear_gradient(nb2_ctx* ctx, const double* dJdu, int32_t precision,
+                               double tolerance, int32_t maximum_iterations, double* dJdG,
+                               int32_t* iterations);
 
 /* ---------------------------------------------------------------------------------------- */
 /* Device-resident stepping (benchmarks and the batched / adjoint harnesses)                */

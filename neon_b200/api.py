@@ -98,6 +98,7 @@ _SIGS = {
     "nb2_update_internal_variables": (C.c_int, [P, P, C.c_double]),
     "nb2_assemble": (C.c_int, [P, P, P]),
     "nb2_save_internal_variables": (C.c_int, [P, C.c_int32]),
+    "nb2_apply_tangent": (C.c_int, [P, P, P]),
     "nb2_get_quadrature_values": (C.c_int, [P, C.c_int32, P]),
     "nb2_apply_dirichlet": (C.c_int, [P, P, C.c_int32, P, P]),
     "nb2_pcg_solve": (C.c_int, [C.c_int32, P, P, P, P, P, C.c_double, C.c_int32,
@@ -112,6 +113,8 @@ _SIGS = {
     "nb2_set_dirichlet_mask": (C.c_int, [P, P, C.c_int32]),
     "nb2_solve_device": (C.c_int, [P, C.c_int32, C.c_double, C.c_int32, C.POINTER(C.c_int32),
                                    C.POINTER(C.c_double)]),
+    "nb2_adjoint_shear_gradient": (C.c_int, [P, P, C.c_int32, C.c_double, C.c_int32, P,
+                                             C.POINTER(C.c_int32)]),
     "nb2_probe_fma_throughput": (C.c_int, [C.c_int32, C.POINTER(C.c_double)]),
 }
 
@@ -205,6 +208,13 @@ class SolidMesh:
         _check(lib().nb2_assemble(self.h, K.ctypes.data, f.ctypes.data), self.h, "assemble")
         return K, f
 
+    def apply_tangent(self, v):
+        """K v, matrix-free, with the tangent of the last update."""
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        y = np.zeros(self.ndofs)
+        _check(lib().nb2_apply_tangent(self.h, v.ctypes.data, y.ctypes.data), self.h, "apply")
+        return y
+
     def save_internal_variables(self, converged: bool):
         _check(lib().nb2_save_internal_variables(self.h, int(bool(converged))), self.h, "save")
 
@@ -257,6 +267,18 @@ class SolidMesh:
 
     def set_stream(self, stream_handle: int):
         _check(lib().nb2_set_stream(self.h, stream_handle), self.h, "set_stream")
+
+    def adjoint_shear_gradient(self, dJdu, precision=FP64, tolerance=1e-12,
+                               maximum_iterations=200000):
+        """dJ/dG_e at the equilibrium of the last StaticMatrix.solve on this mesh."""
+        g = np.ascontiguousarray(dJdu, dtype=np.float64)
+        out = np.zeros(self.conn.shape[0])
+        it = C.c_int32()
+        _check(lib().nb2_adjoint_shear_gradient(self.h, g.ctypes.data, int(precision),
+                                                float(tolerance), int(maximum_iterations),
+                                                out.ctypes.data, C.byref(it)), self.h, "adjoint")
+        self.adjoint_iterations = it.value
+        return out
 
     def launches(self) -> int:
         v = C.c_int64()

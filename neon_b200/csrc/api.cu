@@ -468,6 +468,26 @@ int nb2_synchronize(nb2_ctx* c) {
     return NB2_OK;
 }
 
+int nb2_apply_tangent(nb2_ctx* c, const double* v, double* y) {
+    if (!c || !v || !y) return NB2_E_INPUT;
+    if (!c->dpar) {
+        c->error = "nb2_apply_tangent needs a prior nb2_update_internal_variables";
+        return NB2_E_INPUT;
+    }
+    double *dv = nullptr, *dy = nullptr;
+    NB2_CUDA(c, cudaMallocAsync(&dv, sizeof(double) * c->n, c->stream));
+    NB2_CUDA(c, cudaMallocAsync(&dy, sizeof(double) * c->n, c->stream));
+    NB2_CUDA(c, cudaMemcpyAsync(dv, v, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->stream));
+    int st = launch_apply(c, dv, dy);
+    if (st == NB2_OK)
+        NB2_CUDA(c, cudaMemcpyAsync(y, dy, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
+                                    c->stream));
+    cudaFreeAsync(dv, c->stream);
+    cudaFreeAsync(dy, c->stream);
+    NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    return st;
+}
+
 int nb2_set_dirichlet_mask(nb2_ctx* c, const int32_t* dofs, int32_t nd) {
     if (!c || (nd > 0 && !dofs)) return NB2_E_INPUT;
     for (int i = 0; i < nd; ++i)
@@ -508,6 +528,99 @@ int nb2_solve_device(nb2_ctx* c, int32_t precision, double tol, int32_t maxit, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Mixed-precision solve of K out = rhs (masked rows): FP64 defect correction around FP32 inner
+// PCG solves on K32; the defect rhs - K out applies the FP64 tangent matrix-free (the
+// coefficients stored by the last MODE_STORE element pass), so out converges to the solution of
+// the FP64 system to the relative tolerance `tol`.  rlin, corr, yvec: n-vector work space.
+// ---------------------------------------------------------------------------------------
+static int solve_mixed_system(nb2_ctx* c, const double* rhs, double* out, double tol,
+                              double inner_tol, int maxit, bool graphs, double* rlin,
+                              double* corr, double* yvec, int* iterations) {
+    const unsigned g = grid_for(c->n);
+    const double b2 = device_dot_sync(c, rhs, rhs, c->n);
+    const double thr = std::max(tol * tol * b2, 2.2250738585072014e-308);
+    NB2_CUDA(c, cudaMemsetAsync(out, 0, sizeof(double) * c->n, c->stream));
+    NB2_CUDA(c, cudaMemcpyAsync(rlin, rhs, sizeof(double) * c->n, cudaMemcpyDeviceToDevice,
+                                c->stream));
+    int total = 0;
+    double r2 = b2;
+    for (int ref = 0; ref < 30 && r2 >= thr && b2 > 0; ++ref) {
+        int it = 0;
+        double err = 0;
+        int st = pcg_device_fp32(c, rlin, corr, inner_tol, std::max(1, maxit - total), &it, &err,
+                                 graphs);
+        total += it;
+        if (st && st != NB2_E_CG_MAXIT) {
+            *iterations = total;
+            return st;
+        }
+        k_axpy<<<g, 256, 0, c->stream>>>(c->n, 1.0, corr, out);
+        NB2_TRY(launch_apply(c, out, yvec));
+        k_sub<<<g, 256, 0, c->stream>>>(c->n, rhs, yvec, rlin);
+        k_zero_masked<<<g, 256, 0, c->stream>>>(c->n, c->mask, rlin);
+        c->launches += 3;
+        r2 = device_dot_sync(c, rlin, rlin, c->n);
+        if (total >= maxit) break;
+    }
+    *iterations = total;
+    if (!std::isfinite(r2)) return NB2_E_NAN;
+    if (r2 >= thr && b2 > 0) return NB2_E_CG_MAXIT;
+    return NB2_OK;
+}
+
+// Adjoint gradient of J(u) with respect to the per-element shear modulus of the microsphere
+// model at the context's displacement (the converged state of the last nb2_static_solve, whose
+// Dirichlet mask is still set).  Transpose solve on the tangent (K is symmetric), then
+// dJ/dG_e = -lambda^T df_int/dG_e.
+extern "C" int nb2_adjoint_shear_gradient(nb2_ctx* c, const double* dJdu, int32_t precision,
+                                          double tol, int32_t maxit, double* dJdG,
+                                          int32_t* iterations) {
+    if (!c || !dJdu || !dJdG || maxit <= 0) return NB2_E_INPUT;
+    if (c->mat.model != NB2_GAUSSIAN_AFFINE_MICROSPHERE) {
+        c->error = "the shear-modulus adjoint is defined for the Gaussian affine microsphere";
+        return NB2_E_INPUT;
+    }
+    if (!c->Ge) {  // uniform field = the material modulus
+        std::vector<double> g(c->E, c->mat.shear_modulus);
+        NB2_TRY(nb2_set_element_shear_modulus(c, g.data()));
+    }
+    const bool mixed = precision == NB2_MIXED;
+    NB2_TRY(mixed ? ensure_k32(c) : ensure_k64(c));
+    if (mixed) NB2_TRY(ensure_split_buffers(c));
+    NB2_CUDA(c, cudaMemcpyAsync(c->rhs, dJdu, sizeof(double) * c->n, cudaMemcpyHostToDevice,
+                                c->stream));
+    k_zero_masked<<<grid_for(c->n), 256, 0, c->stream>>>(c->n, c->mask, c->rhs);
+    c->launches++;
+    // tangent at the converged displacement (the microsphere has no history: no state change)
+    NB2_TRY(reset_status(c));
+    int mode = MODE_CONSTITUTIVE | MODE_STIFFNESS | MODE_FORCE | (mixed ? MODE_STORE : 0);
+    NB2_TRY(launch_element_kernel(c, mode, mixed ? NB2_MIXED : NB2_FP64));
+    NB2_TRY(read_status(c));
+    int it = 0;
+    double err = 0;
+    int st;
+    double *rl = nullptr, *co = nullptr, *yv = nullptr, *grad = nullptr;
+    NB2_CUDA(c, cudaMalloc(&grad, sizeof(double) * c->E));
+    if (mixed) {
+        NB2_CUDA(c, cudaMalloc(&rl, sizeof(double) * c->n));
+        NB2_CUDA(c, cudaMalloc(&co, sizeof(double) * c->n));
+        NB2_CUDA(c, cudaMalloc(&yv, sizeof(double) * c->n));
+        st = solve_mixed_system(c, c->rhs, c->du, tol, 1e-4, maxit, true, rl, co, yv, &it);
+    } else {
+        st = pcg_device_fp64(c, c->rhs, c->du, tol, maxit, true, &it, &err, true);
+    }
+    if (iterations) *iterations = it;
+    if (st == NB2_OK) st = launch_adjoint_shear(c, c->du, grad);
+    if (st == NB2_OK) {
+        cudaMemcpyAsync(dJdG, grad, sizeof(double) * c->E, cudaMemcpyDeviceToHost, c->stream);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) st = NB2_E_CUDA;
+    }
+    for (double* p : {rl, co, yv, grad})
+        if (p) cudaFree(p);
+    return st;
+}
 
 // ---------------------------------------------------------------------------------------
 // static_matrix (src/assembler/mechanics/static_matrix.hpp:29-467) over device state
@@ -664,36 +777,9 @@ struct Newton {
     // rlin = rhs - K du uses the FP64 tangent (matrix-free), so du converges to the solution of
     // the same FP64 system as the FP64 path, to the same relative tolerance.
     int solve_mixed(int* iterations) {
-        const double b2 = device_dot_sync(c, c->rhs, c->rhs, c->n);
-        const double thr = std::max(o.cg_tolerance * o.cg_tolerance * b2, 2.2250738585072014e-308);
-        NB2_CUDA(c, cudaMemsetAsync(c->du, 0, sizeof(double) * c->n, c->stream));
-        NB2_CUDA(c, cudaMemcpyAsync(rlin, c->rhs, sizeof(double) * c->n, cudaMemcpyDeviceToDevice,
-                                    c->stream));
-        int total = 0;
-        double r2 = b2;
-        for (int ref = 0; ref < 30 && r2 >= thr && b2 > 0; ++ref) {
-            int it = 0;
-            double err = 0;
-            int st = pcg_device_fp32(c, rlin, corr, o.mixed_inner_tolerance,
-                                     std::max(1, o.cg_maximum_iterations - total), &it, &err,
-                                     o.use_graphs != 0);
-            total += it;
-            if (st && st != NB2_E_CG_MAXIT) {
-                *iterations = total;
-                return st;
-            }
-            k_axpy<<<grid(), 256, 0, c->stream>>>(c->n, 1.0, corr, c->du);
-            NB2_TRY(launch_apply(c, c->du, yvec));
-            k_sub<<<grid(), 256, 0, c->stream>>>(c->n, c->rhs, yvec, rlin);
-            k_zero_masked<<<grid(), 256, 0, c->stream>>>(c->n, c->mask, rlin);
-            c->launches += 3;
-            r2 = device_dot_sync(c, rlin, rlin, c->n);
-            if (total >= o.cg_maximum_iterations) break;
-        }
-        *iterations = total;
-        if (!std::isfinite(r2)) return NB2_E_NAN;
-        if (r2 >= thr && b2 > 0) return NB2_E_CG_MAXIT;
-        return NB2_OK;
+        return solve_mixed_system(c, c->rhs, c->du, o.cg_tolerance, o.mixed_inner_tolerance,
+                                  o.cg_maximum_iterations, o.use_graphs != 0, rlin, corr, yvec,
+                                  iterations);
     }
 
     int solve_linear() {

@@ -387,6 +387,108 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
 }
 
 // ---------------------------------------------------------------------------------------
+// Adjoint gradient with respect to the per-element shear modulus of the Gaussian affine
+// microsphere.  With K lambda = dJ/du solved on the converged tangent,
+//   dJ/dG_e = - lambda^T df_int/dG_e = - sum_q s_q (d sigma_q / dG) : grad(lambda)_q,
+// where sigma = (p I + dev tau)/J and tau = 3 G sum_i w_i t_i (x) t_i (t_i = Fbar r_i), so
+// d sigma/dG = dev(3 sum_i w_i t_i (x) t_i) / J.  The quadrature-point state (F, Fbar, the
+// sphere sum) is recomputed from the displacement, not stored.  One value per element: the
+// group reduces over its points with shuffles, no atomics.
+// ---------------------------------------------------------------------------------------
+template <int NPE>
+__global__ void __launch_bounds__(64) k_adjoint_shear(ElementArgs A, const double* __restrict__ lam,
+                                                      double* __restrict__ dJdG) {
+    using T = Topo<NPE>;
+    constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC;
+    __shared__ double sX[EPC][NPE][3];
+    __shared__ double sx[EPC][NPE][3];
+    __shared__ double sl[EPC][NPE][3];
+    __shared__ double sdN[NQ][NPE][3];
+    const int tid = threadIdx.x;
+    const int le = tid / G;
+    const int lane = tid % G;
+    const long long e = (long long)blockIdx.x * EPC + le;
+    const bool valid = e < A.E;
+    for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
+        (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
+#pragma unroll
+    for (int j = 0; j < (NPE + G - 1) / G; ++j) {
+        const int a = lane + j * G;
+        if (a < NPE && valid) {
+            const int nd = A.conn[e * NPE + a];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double Xv = A.X[3ll * nd + k];
+                sX[le][a][k] = Xv;
+                sx[le][a][k] = A.u[3ll * nd + k] + Xv;
+                sl[le][a][k] = lam[3ll * nd + k];
+            }
+        }
+    }
+    __syncthreads();
+    double contrib = 0.0;
+    const int l = lane;
+    if (valid && l < NQ) {
+        const double w = (NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0);
+        double Fc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, F0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    Fc[i * 3 + k] += sx[le][a][i] * sdN[l][a][k];
+                    F0[i * 3 + k] += sX[le][a][i] * sdN[l][a][k];
+                }
+        double F0i[9], Fd[9], Ji[9];
+        inv3(F0, F0i);
+        matmul3(Fc, F0i, Fd);
+        const double J = det3(Fd);
+        const double sc = pow(J, -1.0 / 3.0);
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 3
+        for (int i = 0; i < 21; ++i) {
+            const double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1],
+                         r2 = c_sphere_r[3 * i + 2], wi = c_sphere_w[i];
+            const double t0 = sc * (Fd[0] * r0 + Fd[1] * r1 + Fd[2] * r2);
+            const double t1 = sc * (Fd[3] * r0 + Fd[4] * r1 + Fd[5] * r2);
+            const double t2 = sc * (Fd[6] * r0 + Fd[7] * r1 + Fd[8] * r2);
+            acc[0] += (t0 * t0) * wi;
+            acc[1] += (t1 * t1) * wi;
+            acc[2] += (t2 * t2) * wi;
+            acc[3] += (t1 * t2) * wi;
+            acc[4] += (t0 * t2) * wi;
+            acc[5] += (t0 * t1) * wi;
+        }
+        // d sigma / dG = dev(3 acc) / J  (11 22 33 23 13 12)
+        const double tr3 = (acc[0] + acc[1] + acc[2]);  // (3 acc) trace / 3
+        double ds[6] = {(3.0 * acc[0] - tr3) / J, (3.0 * acc[1] - tr3) / J,
+                        (3.0 * acc[2] - tr3) / J, 3.0 * acc[3] / J,
+                        3.0 * acc[4] / J,         3.0 * acc[5] / J};
+        inv3(Fc, Ji);
+        const double s = w * det3(Fc);
+        double Gm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+            double La[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                La[k] = sdN[l][a][0] * Ji[0 * 3 + k] + sdN[l][a][1] * Ji[1 * 3 + k] +
+                        sdN[l][a][2] * Ji[2 * 3 + k];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) Gm[i * 3 + k] += sl[le][a][i] * La[k];
+        }
+        contrib = -s * (ds[0] * Gm[0] + ds[1] * Gm[4] + ds[2] * Gm[8] +
+                        ds[3] * (Gm[5] + Gm[7]) + ds[4] * (Gm[2] + Gm[6]) + ds[5] * (Gm[1] + Gm[3]));
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, off);
+    if (valid && lane == 0) dJdG[e] = contrib;
+}
+
+// ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
 static bool g_tables_ready = false;
@@ -495,6 +597,22 @@ int launch_apply(nb2_ctx* c, const double* v, double* y) {
         launch_apply_t<8>(c, A, v, y);
     else
         launch_apply_t<4>(c, A, v, y);
+    NB2_CUDA(c, cudaGetLastError());
+    return NB2_OK;
+}
+
+int launch_adjoint_shear(nb2_ctx* c, const double* lam, double* dJdG) {
+    int st = upload_tables(c);
+    if (st) return st;
+    ElementArgs A = make_args(c);
+    if (c->npe == 8) {
+        constexpr int EPC = Topo<8>::EPC, G = Topo<8>::G;
+        k_adjoint_shear<8><<<(c->E + EPC - 1) / EPC, EPC * G, 0, c->stream>>>(A, lam, dJdG);
+    } else {
+        constexpr int EPC = Topo<4>::EPC, G = Topo<4>::G;
+        k_adjoint_shear<4><<<(c->E + EPC - 1) / EPC, EPC * G, 0, c->stream>>>(A, lam, dJdG);
+    }
+    c->launches++;
     NB2_CUDA(c, cudaGetLastError());
     return NB2_OK;
 }

@@ -149,6 +149,7 @@ int export_csr_values(nb2_ctx* c, const double* Kbsr, double* Kcsr_dev);
 // elements.cu
 int launch_element_kernel(nb2_ctx* c, int mode, int precision);
 int launch_apply(nb2_ctx* c, const double* v, double* y);  // y = K v, FP64 matrix-free
+int launch_adjoint_shear(nb2_ctx* c, const double* lam, double* dJdG);
 void element_flop_model(const nb2_ctx* c, double* flops_per_element);
 
 // pcg.cu

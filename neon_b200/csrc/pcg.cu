@@ -266,7 +266,7 @@ __device__ __forceinline__ void span16(long long b0, long long b1, int size, lon
     hi = (b1 * size + 15) & ~15ll;
 }
 
-template <typename V, typename X>
+template <typename V, typename X, int RPW>
 __global__ void __launch_bounds__(kRedThreads) k_spmv_bulk(Bsr<V> A, BulkPlan plan,
                                                            const X* __restrict__ p,
                                                            X* __restrict__ q,
@@ -338,28 +338,62 @@ __global__ void __launch_bounds__(kRedThreads) k_spmv_bulk(Bsr<V> A, BulkPlan pl
             const long long coff = (cb0 * 4) & 15ll;
             const V* sv = reinterpret_cast<const V*>(stage_base[st] + voff);
             const int* sc = reinterpret_cast<const int*>(stage_base[st] + plan.stage_val_bytes + coff);
-            for (int row = r0 + warp; row < r1; row += nwarps) {
-                const int rb = A.brp[row] - (int)cb0;
-                const int deg = A.brp[row + 1] - A.brp[row];
-                X a0 = 0, a1 = 0, a2 = 0;
-                for (int k = lane; k < deg; k += 32) {
-                    const int col = sc[rb + k];
+            // each warp owns RPW consecutive rows of the chunk and keeps all of them in flight:
+            // block columns and x gathers of every row are issued before any arithmetic
+            const int rbase = r0 + warp * RPW;
+            int rbv[RPW], degv[RPW], colv[RPW];
+            X xv[RPW][3], pv[RPW];
+#pragma unroll
+            for (int t = 0; t < RPW; ++t) {
+                const int row = rbase + t;
+                const bool ok = row < r1;
+                rbv[t] = ok ? A.brp[row] - (int)cb0 : 0;
+                degv[t] = ok ? A.brp[row + 1] - A.brp[row] : 0;
+                colv[t] = lane < degv[t] ? sc[rbv[t] + lane] : 0;
+            }
+#pragma unroll
+            for (int t = 0; t < RPW; ++t) {
+                const bool act = lane < degv[t];
+                xv[t][0] = act ? __ldg(p + 3ll * colv[t]) : (X)0;
+                xv[t][1] = act ? __ldg(p + 3ll * colv[t] + 1) : (X)0;
+                xv[t][2] = act ? __ldg(p + 3ll * colv[t] + 2) : (X)0;
+                pv[t] = (lane < 3 && degv[t] > 0) ? p[3ll * (rbase + t) + lane] : (X)0;
+            }
+            X acc[RPW][3];
+#pragma unroll
+            for (int t = 0; t < RPW; ++t) {
+                acc[t][0] = acc[t][1] = acc[t][2] = (X)0;
+                if (lane < degv[t]) {
+                    const V* blk = sv + 9 * (rbv[t] + lane);
+                    acc[t][0] = (X)blk[0] * xv[t][0] + (X)blk[1] * xv[t][1] + (X)blk[2] * xv[t][2];
+                    acc[t][1] = (X)blk[3] * xv[t][0] + (X)blk[4] * xv[t][1] + (X)blk[5] * xv[t][2];
+                    acc[t][2] = (X)blk[6] * xv[t][0] + (X)blk[7] * xv[t][1] + (X)blk[8] * xv[t][2];
+                }
+                for (int k = lane + 32; k < degv[t]; k += 32) {  // rows of more than 32 blocks
+                    const int col = sc[rbv[t] + k];
                     const X x0 = __ldg(p + 3ll * col), x1 = __ldg(p + 3ll * col + 1),
                             x2 = __ldg(p + 3ll * col + 2);
-                    const V* blk = sv + 9 * (rb + k);
-                    a0 += (X)blk[0] * x0 + (X)blk[1] * x1 + (X)blk[2] * x2;
-                    a1 += (X)blk[3] * x0 + (X)blk[4] * x1 + (X)blk[5] * x2;
-                    a2 += (X)blk[6] * x0 + (X)blk[7] * x1 + (X)blk[8] * x2;
+                    const V* blk = sv + 9 * (rbv[t] + k);
+                    acc[t][0] += (X)blk[0] * x0 + (X)blk[1] * x1 + (X)blk[2] * x2;
+                    acc[t][1] += (X)blk[3] * x0 + (X)blk[4] * x1 + (X)blk[5] * x2;
+                    acc[t][2] += (X)blk[6] * x0 + (X)blk[7] * x1 + (X)blk[8] * x2;
                 }
-                a0 = warp_sum(a0);
-                a1 = warp_sum(a1);
-                a2 = warp_sum(a2);
-                if (lane < 3) {
-                    const long long i = 3ll * row + lane;
-                    X y = lane == 0 ? a0 : (lane == 1 ? a1 : a2);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int t = 0; t < RPW; ++t)
+#pragma unroll
+                    for (int r = 0; r < 3; ++r)
+                        acc[t][r] += __shfl_xor_sync(0xffffffffu, acc[t][r], o);
+#pragma unroll
+            for (int t = 0; t < RPW; ++t) {
+                if (lane < 3 && degv[t] > 0) {
+                    const long long i = 3ll * (rbase + t) + lane;
+                    X y = lane == 0 ? acc[t][0] : (lane == 1 ? acc[t][1] : acc[t][2]);
                     if (mask && mask[i]) y = (X)0;
                     q[i] = y;
-                    dot[0] += (double)p[i] * (double)y;
+                    dot[0] += (double)pv[t] * (double)y;
                 }
             }
         }
@@ -613,13 +647,14 @@ static int wait_scalars(nb2_ctx* c) {
 }
 
 constexpr int kChunk = 32;
-constexpr int kBulkSmemBudget = 110 * 1024;  // per CTA: two CTAs per SM
-constexpr int kBulkCtasPerSm = 2;
+constexpr int kBulkSmemBudget = 200 * 1024;  // per CTA
+constexpr int kBulkWarps = kRedThreads / 32;
 
-// Rows per chunk and stage sizes of the bulk SpMV: the largest power-of-two chunk whose
-// kStages stages fit the shared-memory budget (spans widened to 16 B as the copies are).
+// Rows per chunk and stage sizes of the bulk SpMV: 8 warps x RPW rows with the largest RPW in
+// {8, 4, 2, 1} whose kStages stages fit the shared-memory budget (spans widened to 16 B as the
+// copies are).
 static bool make_bulk_plan(const nb2_ctx* c, int vsize, BulkPlan* plan) {
-    for (int R = 64; R >= 2; R /= 2) {
+    for (int R = 8 * kBulkWarps; R >= kBulkWarps; R /= 2) {
         long long maxv = 0, maxc = 0;
         const int chunks = (c->N + R - 1) / R;
         for (int ch = 0; ch < chunks; ++ch) {
@@ -648,12 +683,22 @@ static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv,
     const bool bulk = make_bulk_plan(c, (int)sizeof(V), &plan);
     int bulk_grid = 0;
     size_t bulk_smem = 0;
+    const int rpw = bulk ? plan.rows_per_chunk / kBulkWarps : 0;
+    auto bulk_kernel = [&]() -> void (*)(Bsr<V>, BulkPlan, const X*, X*, const unsigned char*,
+                                         CgScalars*, double*) {
+        switch (rpw) {
+            case 8: return k_spmv_bulk<V, X, 8>;
+            case 4: return k_spmv_bulk<V, X, 4>;
+            case 2: return k_spmv_bulk<V, X, 2>;
+            default: return k_spmv_bulk<V, X, 1>;
+        }
+    }();
     if (bulk) {
         bulk_smem = (size_t)kStages * (plan.stage_val_bytes + plan.stage_col_bytes);
-        NB2_CUDA(c, cudaFuncSetAttribute(k_spmv_bulk<V, X>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+        NB2_CUDA(c, cudaFuncSetAttribute(bulk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)bulk_smem));
-        bulk_grid = std::min(plan.chunks, 148 * kBulkCtasPerSm);
+        const int per_sm = std::max(1, (int)((220 * 1024) / (bulk_smem + 4096)));
+        bulk_grid = std::min(plan.chunks, 148 * per_sm);
     }
     const long long n = c->n;
     k_invdiag<V, X><<<(c->N + 255) / 256, 256, 0, c->stream>>>(A, inv);
@@ -666,8 +711,8 @@ static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv,
     auto enqueue = [&](int count) {
         for (int it = 0; it < count; ++it) {
             if (bulk)
-                k_spmv_bulk<V, X><<<bulk_grid, kRedThreads, bulk_smem, c->stream>>>(
-                    A, plan, p, q, mask, c->cgs, c->partials);
+                bulk_kernel<<<bulk_grid, kRedThreads, bulk_smem, c->stream>>>(A, plan, p, q, mask,
+                                                                              c->cgs, c->partials);
             else
                 k_spmv<V, X><<<RB, kRedThreads, 0, c->stream>>>(A, p, q, mask, c->cgs,
                                                                 c->partials);

@@ -1,0 +1,87 @@
+"""Adjoint gradient of the microsphere problem (config 4 shape, small mesh): against central
+finite differences of the forward solve and against the mixed-precision adjoint; the
+torch.autograd harness gives the same gradient."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from neon_b200 import problem as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(n=4, seed=7):
+    pr = P.config_c4(n, seed_field=seed)
+    o = pr.options
+    o.residual_tolerance = o.displacement_tolerance = 1e-13
+    o.cg_tolerance = 1e-13
+    o.linear_iterations = 25
+    return pr
+
+
+def _objective(pr, u, u_target):
+    top = np.unique(pr.mesh.faces["top"].reshape(-1))
+    dofs = (3 * top[:, None] + np.arange(3)).reshape(-1)
+    d = u[dofs] - u_target[dofs]
+    g = np.zeros_like(u)
+    g[dofs] = d
+    return 0.5 * float(d @ d), g
+
+
+@pytest.fixture(scope="module")
+def setup():
+    from neon_b200 import api, build
+    build.build()
+    pr = _problem()
+    target = P.config_c4(4, seed_field=99)
+    u_target = api.StaticMatrix(target).solve()
+    return api, pr, u_target
+
+
+def test_adjoint_matches_central_differences(setup):
+    api, pr, u_target = setup
+    sm = api.StaticMatrix(pr)
+    u = sm.solve()
+    J, g = _objective(pr, u, u_target)
+    grad = sm.mesh.adjoint_shear_gradient(g, api.FP64, 1e-13)
+    rng = np.random.Generator(np.random.PCG64(3))
+    picks = rng.choice(pr.mesh.num_elements, size=8, replace=False)
+    G0 = pr.element_shear_modulus.copy()
+    for e in picks:
+        h = 1e-4 * G0[e]
+        vals = []
+        for sgn in (1.0, -1.0):
+            pr.element_shear_modulus = G0.copy()
+            pr.element_shear_modulus[e] += sgn * h
+            up = api.StaticMatrix(pr).solve()
+            vals.append(_objective(pr, up, u_target)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(grad[e] - fd) <= 1e-5 * abs(fd) + 1e-9 * np.abs(grad).max(), (e, grad[e], fd)
+    pr.element_shear_modulus = G0
+
+
+def test_mixed_adjoint_matches_fp64(setup):
+    api, pr, u_target = setup
+    sm = api.StaticMatrix(pr)
+    u = sm.solve()
+    _, g = _objective(pr, u, u_target)
+    g64 = sm.mesh.adjoint_shear_gradient(g, api.FP64, 1e-12)
+    g32 = sm.mesh.adjoint_shear_gradient(g, api.MIXED, 1e-12)
+    assert rel_err(g32, g64) < 1e-9
+
+
+def test_torch_autograd_harness(setup):
+    import torch
+    from neon_b200.autograd import equilibrium_displacement
+    api, pr, u_target = setup
+    G = torch.tensor(pr.element_shear_modulus, dtype=torch.float64, requires_grad=True)
+    u = equilibrium_displacement(G, pr)
+    top = np.unique(pr.mesh.faces["top"].reshape(-1))
+    dofs = torch.from_numpy((3 * top[:, None] + np.arange(3)).reshape(-1))
+    d = u[dofs] - torch.from_numpy(u_target)[dofs]
+    J = 0.5 * (d * d).sum()
+    J.backward()
+    sm = api.StaticMatrix(pr)
+    _, g = _objective(pr, sm.solve(), u_target)
+    ref = sm.mesh.adjoint_shear_gradient(g, api.FP64, 1e-12)
+    assert rel_err(G.grad.numpy(), ref) < 1e-10
