@@ -115,6 +115,8 @@ _SIGS = {
                                    C.POINTER(C.c_double)]),
     "nb2_adjoint_shear_gradient": (C.c_int, [P, P, C.c_int32, C.c_double, C.c_int32, P,
                                              C.POINTER(C.c_int32)]),
+    "nb2_pcg_solve_noalloc": (C.c_int, [C.c_int32, P, P, P, P, P, C.c_double, C.c_int32, P,
+                                        C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "nb2_probe_fma_throughput": (C.c_int, [C.c_int32, C.POINTER(C.c_double)]),
 }
 

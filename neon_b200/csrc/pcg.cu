@@ -918,4 +918,102 @@ done:
     return status;
 }
 
+// ---------------------------------------------------------------------------------------
+// Allocation-free PCG (nb2_pcg_solve_noalloc).
+//
+// For callers that must not allocate device memory while they run a solve -- a code that
+// places every device byte itself through its own pool or arena and forbids hidden
+// allocations, a host thread that issues work while another thread captures a stream, or a
+// long-running service that must not trigger allocator growth or device synchronisation in
+// the middle of a time step.  They pass the matrix, right-hand side and solution in device
+// memory they own; the solver's own work vectors, reduction partials and scalars live in the
+// fixed array below, which every GPU that loads this library holds until the process exits.
+// ---------------------------------------------------------------------------------------
+constexpr int kNoAllocMaxRows = NB2_NOALLOC_MAX_ROWS;
+constexpr int kNoAllocBlocks = 148 * 4;
+// layout (doubles): [partials kNoAllocBlocks*8][scalars 32][r][p][q][inv] (rows each)
+constexpr size_t kNoAllocPartials = (size_t)kNoAllocBlocks * 8;
+constexpr size_t kNoAllocScalars = 32;  // >= sizeof(CgScalars) / 8, keeps 256-byte alignment
+constexpr size_t kNoAllocDoubles = kNoAllocPartials + kNoAllocScalars + 4ull * kNoAllocMaxRows;
+static_assert(sizeof(CgScalars) <= kNoAllocScalars * sizeof(double), "scalar slot too small");
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+// row pointers monotone from 0, column indices in range; flag[0] = 1 on any violation
+__global__ void k_check_csr(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                            unsigned int* flag) {
+    const long long nnz = rp[n];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        if (rp[i + 1] < rp[i] || rp[i] < 0 || rp[i + 1] > nnz) atomicOr(flag, 1u);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && rp[0] != 0) atomicOr(flag, 1u);
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+         k += (long long)gridDim.x * blockDim.x)
+        if (ci[k] < 0 || ci[k] >= n) atomicOr(flag, 1u);
+}
+
 }  // namespace nb2
+
+extern "C" int nb2_pcg_solve_noalloc(int32_t n, const int32_t* rowptr, const int32_t* col,
+                                     const double* values, const double* b, double* x,
+                                     double tolerance, int32_t maximum_iterations, void* stream,
+                                     int32_t* iterations, double* error) {
+    using namespace nb2;
+    if (n <= 0 || !rowptr || !col || !values || !b || !x || maximum_iterations <= 0)
+        return NB2_E_INPUT;
+    if (n > kNoAllocMaxRows) return NB2_E_INPUT;  // beyond the fixed workspace
+    // device address of the fixed workspace, looked up once per device with that device
+    // current (the symbol's host-side name is not a device address)
+    static double* scratch_of_device[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return NB2_E_CUDA;
+    if (!scratch_of_device[dev]) {
+        void* ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
+            return NB2_E_CUDA;
+        scratch_of_device[dev] = static_cast<double*>(ptr);
+    }
+    double* base = scratch_of_device[dev];
+    double* partials = base;
+    CgScalars* s = reinterpret_cast<CgScalars*>(base + kNoAllocPartials);
+    double* r = base + kNoAllocPartials + kNoAllocScalars;
+    double* p = r + kNoAllocMaxRows;
+    double* q = p + kNoAllocMaxRows;
+    double* inv = q + kNoAllocMaxRows;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int RB = kNoAllocBlocks;
+    // the workspace keeps the previous call's contents: the scalars (reduction tickets, flags)
+    // must start at zero
+    if (cudaMemsetAsync(s, 0, sizeof(CgScalars), st) != cudaSuccess) return NB2_E_CUDA;
+    unsigned int* flag = &s->counter[3];
+    k_check_csr<<<RB, kRedThreads, 0, st>>>(n, rowptr, col, flag);
+    CgScalars hs;
+    if (cudaMemcpyAsync(&hs, s, sizeof hs, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return NB2_E_CUDA;
+    if (hs.counter[3] != 0) return NB2_E_INPUT;
+    if (cudaMemsetAsync(s, 0, sizeof(CgScalars), st) != cudaSuccess) return NB2_E_CUDA;
+    if (cudaMemcpyAsync(&s->max_iterations, &maximum_iterations, sizeof(int),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return NB2_E_CUDA;
+    Csr A{rowptr, col, values, n};
+    k_csr_invdiag<<<(n + 255) / 256, 256, 0, st>>>(A, inv);
+    k_init<double><<<RB, kRedThreads, 0, st>>>(n, b, x, r, p, inv, s, partials, tolerance);
+    int guard = 0;
+    for (;;) {
+        if (++guard > maximum_iterations / kChunk + 4) return NB2_E_TIMEOUT;
+        for (int it = 0; it < kChunk; ++it) {
+            k_csr_spmv<<<RB, kRedThreads, 0, st>>>(A, p, q, s, partials);
+            k_xr<double><<<RB, kRedThreads, 0, st>>>(n, x, r, p, q, inv, s, partials);
+            k_p<double><<<RB, kRedThreads, 0, st>>>(n, p, r, inv, s);
+        }
+        if (cudaMemcpyAsync(&hs, s, sizeof hs, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return NB2_E_CUDA;
+        if (hs.done) break;
+    }
+    if (cudaGetLastError() != cudaSuccess) return NB2_E_CUDA;
+    if (iterations) *iterations = hs.iterations;
+    if (error) *error = hs.rhs_norm2 > 0 ? std::sqrt(hs.rr / hs.rhs_norm2) : 0.0;
+    return hs.status ? hs.status : NB2_OK;
+}
