@@ -152,6 +152,11 @@ int nb2_launch_count(const nb2_ctx* ctx, int64_t* launches);
 
 /* Per-element shear modulus (replaces the material G of the microsphere model per element). */
 int nb2_set_element_shear_modulus(nb2_ctx* ctx, const double* shear_modulus);
+/* Per-element bulk and shear modulus ([num_elements] each, either may be NULL) replacing the
+ * material's K, G (lambda = K - 2G/3) for linear elasticity, neo-Hooke and the microsphere:
+ * element groups of different materials (neon builds one submesh and one constitutive model per
+ * group, mesh.cpp:36-42) in a single context, as the batched solves do. */
+int nb2_set_element_moduli(nb2_ctx* ctx, const double* bulk_modulus, const double* shear_modulus);
 
 /* ---------------------------------------------------------------------------------------- */
 /* Element-level drop-ins (host buffers)                                                   */
@@ -267,6 +272,34 @@ int nb2_set_dirichlet_mask(nb2_ctx* ctx, const int32_t* dofs, int32_t num_dofs);
  * tolerance 0 runs exactly maximum_iterations iterations (timing). */
 int nb2_solve_device(nb2_ctx* ctx, int32_t precision, double tolerance, int32_t maximum_iterations,
                      int32_t* iterations, double* error);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Batched solves: many independent problems of uneven size in one context                  */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Static solves of num_instances independent problems that share one context (one model; each
+ * instance's moduli set per element with nb2_set_element_moduli).  Instance i owns the nodes
+ * [node_offsets[i], node_offsets[i+1]) and the elements on them (an element that couples two
+ * instances is NB2_E_INPUT); its Dirichlet tables are dirichlet[dirichlet_offsets[i] ..
+ * dirichlet_offsets[i+1]) and its nodal-force tables nodal_forces[force_offsets[i] ..
+ * force_offsets[i+1]), DOFs global.  Every instance runs static_matrix::solve
+ * (static_matrix.hpp:145-187, 402-467) with its own load stepping, Newton norms, cutbacks and
+ * Jacobi-PCG (linear_solver.cpp:67-109), as if solved alone; one element pass, SpMV and vector
+ * update serves all instances per launch.  options apply to every instance (precision NB2_FP64
+ * or NB2_MIXED).  Models without history only (no J2 plasticity).  reports: [num_instances];
+ * log (nullable): [num_instances][max_log].  Returns the first failing instance's status.
+ * neon solves one mesh per simulation: no counterpart interface. */
+int nb2_batch_static_solve(nb2_ctx* ctx, int32_t num_instances, const int32_t* node_offsets,
+                           const nb2_solver_options* options, const nb2_dof_table* dirichlet,
+                           const int32_t* dirichlet_offsets, const nb2_dof_table* nodal_forces,
+                           const int32_t* force_offsets, double* u_out,
+                           nb2_solve_report* reports, nb2_newton_log* log, int32_t max_log);
+/* Autotuner of the batched PCG: times the SpMV over the instances' rows for each rows-per-chunk
+ * (16, 32, 64, 128) and lanes-per-block-row (4, 8, 16, 32) candidate on this device and keeps
+ * the fastest for the context's next nb2_batch_static_solve.  No counterpart in the reference. */
+int nb2_batch_autotune(nb2_ctx* ctx, int32_t num_instances, const int32_t* node_offsets,
+                       int32_t precision, int32_t* rows_per_chunk, int32_t* lanes_per_row,
+                       double* ms_per_spmv);
 
 #ifdef __cplusplus
 }

@@ -94,6 +94,7 @@ _SIGS = {
                                 C.POINTER(C.c_int64)]),
     "nb2_launch_count": (C.c_int, [P, C.POINTER(C.c_int64)]),
     "nb2_set_element_shear_modulus": (C.c_int, [P, P]),
+    "nb2_set_element_moduli": (C.c_int, [P, P, P]),
     "nb2_export_pattern": (C.c_int, [P, P, P]),
     "nb2_update_internal_variables": (C.c_int, [P, P, C.c_double]),
     "nb2_assemble": (C.c_int, [P, P, P]),
@@ -118,6 +119,10 @@ _SIGS = {
     "nb2_pcg_solve_noalloc": (C.c_int, [C.c_int32, P, P, P, P, P, C.c_double, C.c_int32, P,
                                         C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "nb2_probe_fma_throughput": (C.c_int, [C.c_int32, C.POINTER(C.c_double)]),
+    "nb2_batch_static_solve": (C.c_int, [P, C.c_int32, P, C.POINTER(SolverOptions), P, P, P, P,
+                                         P, P, P, C.c_int32]),
+    "nb2_batch_autotune": (C.c_int, [P, C.c_int32, P, C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
 }
 
 _lib = None
@@ -181,6 +186,14 @@ class SolidMesh:
         if element_shear_modulus is not None:
             g = np.ascontiguousarray(element_shear_modulus, dtype=np.float64)
             _check(L.nb2_set_element_shear_modulus(self.h, g.ctypes.data), self.h, "shear")
+
+    def set_element_moduli(self, bulk_modulus=None, shear_modulus=None):
+        """Per-element K and G ([num_elements] each, either may be None) in place of the
+        material's (linear elasticity, neo-Hooke, microsphere)."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                for a in (bulk_modulus, shear_modulus)]
+        ptr = [None if a is None else a.ctypes.data for a in arrs]
+        _check(lib().nb2_set_element_moduli(self.h, ptr[0], ptr[1]), self.h, "moduli")
 
     def close(self):
         if getattr(self, "h", None):
@@ -384,3 +397,126 @@ class StaticMatrix:
                 raise ComputationalError(st, self.report["message"])
             _check(st, self.mesh.h, "static_solve")
         return u
+
+
+def batch_layout(problems):
+    """The block-diagonal mesh of a batch: concatenated coordinates, connectivity shifted by each
+    instance's node offset, per-element K and G, and every boundary table with its DOFs shifted
+    to the global numbering (tables of instance i at [offsets[i], offsets[i+1]))."""
+    if not problems:
+        raise ValueError("no problems")
+    model = problems[0].material.model
+    npe = problems[0].mesh.conn.shape[1]
+    for pr in problems:
+        if pr.material.model != model or pr.mesh.conn.shape[1] != npe:
+            raise ValueError("batched problems share one model and one element type")
+    node_offsets = np.zeros(len(problems) + 1, np.int32)
+    Xs, conns, Ks, Gs = [], [], [], []
+    tables = {"dirichlet": ([], [0]), "nodal_forces": ([], [0])}
+    for i, pr in enumerate(problems):
+        off = int(node_offsets[i])
+        Xs.append(pr.mesh.X)
+        conns.append(pr.mesh.conn + off)
+        E = pr.mesh.conn.shape[0]
+        Ks.append(np.full(E, pr.material.K))
+        Gs.append(pr.element_shear_modulus if pr.element_shear_modulus is not None
+                  else np.full(E, pr.material.G))
+        node_offsets[i + 1] = off + pr.mesh.num_nodes
+        for which, (lst, offs) in tables.items():
+            for t in getattr(pr, which):
+                lst.append(type(t)(np.asarray(t.dofs, np.int64) + 3 * off, t.times, t.values,
+                                   t.weights, t.name))
+            offs.append(len(lst))
+    if 3 * int(node_offsets[-1]) >= 2 ** 31:
+        raise ValueError("the batch has more DOFs than int32 indices address")
+    return {"X": np.concatenate(Xs), "conn": np.concatenate(conns).astype(np.int32),
+            "K": np.concatenate(Ks), "G": np.concatenate(Gs), "node_offsets": node_offsets,
+            "element_offsets": np.concatenate([[0], np.cumsum([c.shape[0] for c in conns])]),
+            "dirichlet": tables["dirichlet"][0],
+            "dirichlet_offsets": np.asarray(tables["dirichlet"][1], np.int32),
+            "nodal_forces": tables["nodal_forces"][0],
+            "force_offsets": np.asarray(tables["nodal_forces"][1], np.int32)}
+
+
+class BatchedStaticMatrix:
+    """Many independent static_matrix solves of uneven size in one context: the instances'
+    meshes are concatenated into one block-diagonal mesh, each instance keeps its own material
+    (per-element moduli), boundary tables, load stepping, Newton decisions and PCG.  All problems
+    share one constitutive model and one set of solver options (those of the first problem)."""
+
+    def __init__(self, problems, precision=FP64, mixed_inner_tolerance=1e-4, use_graphs=True,
+                 autotune=True):
+        self.problems = list(problems)
+        self.layout = batch_layout(self.problems)
+        lay = self.layout
+        self.node_offsets = lay["node_offsets"]
+        self.element_offsets = lay["element_offsets"]
+        self.mesh = SolidMesh(lay["X"], lay["conn"], self.problems[0].material)
+        self.mesh.set_element_moduli(lay["K"], lay["G"])
+        o = problems[0].options
+        self.options = SolverOptions(o.residual_tolerance, o.displacement_tolerance,
+                                     o.linear_iterations, int(o.absolute_tolerance), o.period,
+                                     o.initial, o.minimum, o.maximum, int(o.adaptive),
+                                     o.cg_tolerance, o.cg_maximum_iterations, int(precision),
+                                     mixed_inner_tolerance, int(bool(use_graphs)))
+        self.precision = precision
+        self.tuned = None
+        if autotune:
+            self.autotune()
+        self.reports = None
+        self.logs = None
+        self.displacement = None
+
+    @property
+    def num_instances(self):
+        return len(self.problems)
+
+    def autotune(self):
+        """Pick the batched PCG's rows per chunk and lanes per block row by timing."""
+        R, L, ms = C.c_int32(), C.c_int32(), C.c_double()
+        _check(lib().nb2_batch_autotune(self.mesh.h, self.num_instances,
+                                        self.node_offsets.ctypes.data, int(self.precision),
+                                        C.byref(R), C.byref(L), C.byref(ms)), self.mesh.h,
+               "autotune")
+        self.tuned = {"rows_per_chunk": R.value, "lanes_per_row": L.value, "ms_per_spmv": ms.value}
+        return self.tuned
+
+    def solve(self, max_log=64, raise_on_error=True):
+        keep = []
+        lay = self.layout
+        dir_t, dir_off = lay["dirichlet"], lay["dirichlet_offsets"]
+        frc_t, frc_off = lay["nodal_forces"], lay["force_offsets"]
+        dt = _tables(dir_t, keep)
+        nf = _tables(frc_t, keep)
+        n = self.num_instances
+        u = np.zeros(self.mesh.ndofs)
+        reps = (SolveReport * n)()
+        log = (NewtonLog * (n * max_log))()
+        st = lib().nb2_batch_static_solve(self.mesh.h, n, self.node_offsets.ctypes.data,
+                                          C.byref(self.options), C.cast(dt, P),
+                                          dir_off.ctypes.data, C.cast(nf, P), frc_off.ctypes.data,
+                                          u.ctypes.data, C.cast(reps, P), C.cast(log, P), max_log)
+        self.displacement = u
+        self.reports = []
+        self.logs = []
+        for i in range(n):
+            r = {k: getattr(reps[i], k) for k, _ in SolveReport._fields_}
+            r["message"] = reps[i].message.decode()
+            self.reports.append(r)
+            m = min(int(r["newton_iterations"]), max_log)
+            self.logs.append(np.array([[log[i * max_log + j].step_time,
+                                        log[i * max_log + j].iteration,
+                                        log[i * max_log + j].cg_iterations,
+                                        log[i * max_log + j].displacement_norm,
+                                        log[i * max_log + j].force_norm] for j in range(m)]))
+        if raise_on_error and st != OK:
+            if st in RECOVERABLE or st == E_CUTBACK_LIMIT:
+                bad = [i for i, r in enumerate(self.reports) if r["status"] != OK]
+                raise ComputationalError(st, "instance %s: %s" % (
+                    bad[:1], self.reports[bad[0]]["message"] if bad else ""))
+            _check(st, self.mesh.h, "batch_static_solve")
+        return u
+
+    def instance_displacement(self, i, u=None):
+        u = self.displacement if u is None else u
+        return u[3 * self.node_offsets[i]:3 * self.node_offsets[i + 1]]

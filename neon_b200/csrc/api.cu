@@ -3,6 +3,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -71,13 +72,13 @@ using namespace nb2;
 // ---------------------------------------------------------------------------------------
 // status word -> neon's computational_error messages
 // ---------------------------------------------------------------------------------------
-static int reset_status(nb2_ctx* c) {
+int nb2::reset_status(nb2_ctx* c) {
     DeviceStatus z{0u, 0u, ~0ull};
     NB2_CUDA(c, cudaMemcpyAsync(c->status, &z, sizeof z, cudaMemcpyHostToDevice, c->stream));
     return NB2_OK;
 }
 
-static int read_status(nb2_ctx* c) {
+int nb2::read_status(nb2_ctx* c) {
     DeviceStatus h;
     NB2_CUDA(c, cudaMemcpyAsync(&h, c->status, sizeof h, cudaMemcpyDeviceToHost, c->stream));
     NB2_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -110,21 +111,16 @@ static int dev_alloc(nb2_ctx* c, T** p, long long count) {
     return NB2_OK;
 }
 
-#define NB2_TRY(x)                   \
-    do {                             \
-        int _s = (x);                \
-        if (_s != NB2_OK) return _s; \
-    } while (0)
-
-static int ensure_split_buffers(nb2_ctx* c) {
+int nb2::ensure_split_buffers(nb2_ctx* c) {
     if (c->sig) return NB2_OK;
     NB2_TRY(dev_alloc(c, &c->sig, 6ll * c->nqp));
     NB2_TRY(dev_alloc(c, &c->dpar, 9ll * c->nqp));
     NB2_TRY(dev_alloc(c, &c->detF, (long long)c->nqp));
+    NB2_TRY(dev_alloc(c, &c->u_tan, (long long)c->n));
     return NB2_OK;
 }
 
-static int ensure_k32(nb2_ctx* c) {
+int nb2::ensure_k32(nb2_ctx* c) {
     if (c->K32) return NB2_OK;
     // +16 B: the bulk SpMV widens every copy to 16-byte boundaries
     NB2_TRY(dev_alloc(c, &c->K32, 9 * c->nnzb + 4));
@@ -136,7 +132,7 @@ static int ensure_k32(nb2_ctx* c) {
     return NB2_OK;
 }
 
-static int ensure_k64(nb2_ctx* c) {
+int nb2::ensure_k64(nb2_ctx* c) {
     if (c->K64) return NB2_OK;
     return dev_alloc(c, &c->K64, 9 * c->nnzb + 2);  // +16 B for the bulk SpMV spans
 }
@@ -221,7 +217,8 @@ int nb2_destroy(nb2_ctx* c) {
     release_graphs(c);
     void* ptrs[] = {c->X,      c->conn,   c->brp,    c->bcol,   c->slot,      c->K64,
                     c->K32,    c->u,      c->u_old,  c->fint,   c->fext,      c->rhs,
-                    c->du,     c->inc,    c->mask,   c->Ge,     c->ep,        c->epbar,
+                    c->du,     c->inc,    c->mask,   c->Ge,     c->Ke,        c->ep,
+                    c->epbar,  c->u_tan,
                     c->ep_old, c->epbar_old, c->sig, c->dpar,   c->detF,      c->cg_x,
                     c->cg_r,   c->cg_p,   c->cg_q,   c->cg_inv, c->cg32_x,    c->cg32_r,
                     c->cg32_p, c->cg32_q, c->cg32_inv, c->partials, c->cgs,   c->norms,
@@ -271,6 +268,22 @@ int nb2_set_element_shear_modulus(nb2_ctx* c, const double* G) {
     if (!c->Ge) NB2_TRY(dev_alloc(c, &c->Ge, (long long)c->E));
     NB2_CUDA(c, cudaMemcpyAsync(c->Ge, G, sizeof(double) * c->E, cudaMemcpyHostToDevice, c->stream));
     NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    return NB2_OK;
+}
+
+int nb2_set_element_moduli(nb2_ctx* c, const double* K, const double* G) {
+    if (!c || (!K && !G)) return NB2_E_INPUT;
+    if (c->mat.model == NB2_SMALL_STRAIN_J2_PLASTICITY) {
+        c->error = "per-element moduli are not supported for J2 plasticity";
+        return NB2_E_INPUT;
+    }
+    if (G) NB2_TRY(nb2_set_element_shear_modulus(c, G));
+    if (K) {
+        if (!c->Ke) NB2_TRY(dev_alloc(c, &c->Ke, (long long)c->E));
+        NB2_CUDA(c, cudaMemcpyAsync(c->Ke, K, sizeof(double) * c->E, cudaMemcpyHostToDevice,
+                                    c->stream));
+        NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
     return NB2_OK;
 }
 
@@ -535,9 +548,24 @@ int nb2_solve_device(nb2_ctx* c, int32_t precision, double tol, int32_t maxit, i
 // coefficients stored by the last MODE_STORE element pass), so out converges to the solution of
 // the FP64 system to the relative tolerance `tol`.  rlin, corr, yvec: n-vector work space.
 // ---------------------------------------------------------------------------------------
+// inner: NB2_MIXED (FP32 K32 inner PCG) or NB2_FP64 (K64); exact: the defect uses the exact
+// forward-mode product (d f_int/du) v instead of the stored (assembled) tangent.
+static int solve_defect_corrected(nb2_ctx* c, const double* rhs, double* out, double tol,
+                                  double inner_tol, int maxit, bool graphs, double* rlin,
+                                  double* corr, double* yvec, int* iterations, int inner,
+                                  bool exact);
+
 static int solve_mixed_system(nb2_ctx* c, const double* rhs, double* out, double tol,
                               double inner_tol, int maxit, bool graphs, double* rlin,
                               double* corr, double* yvec, int* iterations) {
+    return solve_defect_corrected(c, rhs, out, tol, inner_tol, maxit, graphs, rlin, corr, yvec,
+                                  iterations, NB2_MIXED, false);
+}
+
+static int solve_defect_corrected(nb2_ctx* c, const double* rhs, double* out, double tol,
+                                  double inner_tol, int maxit, bool graphs, double* rlin,
+                                  double* corr, double* yvec, int* iterations, int inner,
+                                  bool exact) {
     const unsigned g = grid_for(c->n);
     const double b2 = device_dot_sync(c, rhs, rhs, c->n);
     const double thr = std::max(tol * tol * b2, 2.2250738585072014e-308);
@@ -549,19 +577,28 @@ static int solve_mixed_system(nb2_ctx* c, const double* rhs, double* out, double
     for (int ref = 0; ref < 30 && r2 >= thr && b2 > 0; ++ref) {
         int it = 0;
         double err = 0;
-        int st = pcg_device_fp32(c, rlin, corr, inner_tol, std::max(1, maxit - total), &it, &err,
-                                 graphs);
+        int st = inner == NB2_FP64
+                     ? pcg_device_fp64(c, rlin, corr, inner_tol, std::max(1, maxit - total), true,
+                                       &it, &err, graphs)
+                     : pcg_device_fp32(c, rlin, corr, inner_tol, std::max(1, maxit - total), &it,
+                                       &err, graphs);
         total += it;
         if (st && st != NB2_E_CG_MAXIT) {
             *iterations = total;
             return st;
         }
         k_axpy<<<g, 256, 0, c->stream>>>(c->n, 1.0, corr, out);
-        NB2_TRY(launch_apply(c, out, yvec));
+        if (exact)
+            NB2_TRY(launch_force_jvp(c, out, yvec));
+        else
+            NB2_TRY(launch_apply(c, out, yvec));
         k_sub<<<g, 256, 0, c->stream>>>(c->n, rhs, yvec, rlin);
         k_zero_masked<<<g, 256, 0, c->stream>>>(c->n, c->mask, rlin);
         c->launches += 3;
         r2 = device_dot_sync(c, rlin, rlin, c->n);
+        if (std::getenv("NB2_DEBUG"))
+            std::fprintf(stderr, "[nb2] defect correction %d: inner its %d (status %d) |r|^2 %.6e "
+                         "b^2 %.6e threshold %.6e\n", ref, it, st, r2, b2, thr);
         if (total >= maxit) break;
     }
     *iterations = total;
@@ -599,18 +636,17 @@ extern "C" int nb2_adjoint_shear_gradient(nb2_ctx* c, const double* dJdu, int32_
     NB2_TRY(launch_element_kernel(c, mode, mixed ? NB2_MIXED : NB2_FP64));
     NB2_TRY(read_status(c));
     int it = 0;
-    double err = 0;
     int st;
     double *rl = nullptr, *co = nullptr, *yv = nullptr, *grad = nullptr;
     NB2_CUDA(c, cudaMalloc(&grad, sizeof(double) * c->E));
-    if (mixed) {
-        NB2_CUDA(c, cudaMalloc(&rl, sizeof(double) * c->n));
-        NB2_CUDA(c, cudaMalloc(&co, sizeof(double) * c->n));
-        NB2_CUDA(c, cudaMalloc(&yv, sizeof(double) * c->n));
-        st = solve_mixed_system(c, c->rhs, c->du, tol, 1e-4, maxit, true, rl, co, yv, &it);
-    } else {
-        st = pcg_device_fp64(c, c->rhs, c->du, tol, maxit, true, &it, &err, true);
-    }
+    NB2_CUDA(c, cudaMalloc(&rl, sizeof(double) * c->n));
+    NB2_CUDA(c, cudaMalloc(&co, sizeof(double) * c->n));
+    NB2_CUDA(c, cudaMalloc(&yv, sizeof(double) * c->n));
+    // neon's assembled tangent is not the exact derivative of f_int: solve the exact system by
+    // defect correction, the assembled K (FP64, or FP32 for the mixed adjoint) as inner solver
+    // and the forward-mode product (d f_int/du) lambda as residual
+    st = solve_defect_corrected(c, c->rhs, c->du, tol, mixed ? 1e-4 : 1e-6, maxit, true, rl, co,
+                                yv, &it, mixed ? NB2_MIXED : NB2_FP64, true);
     if (iterations) *iterations = it;
     if (st == NB2_OK) st = launch_adjoint_shear(c, c->du, grad);
     if (st == NB2_OK) {

@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : 8) k_element(Ele
     const int le = tid / G;
     const int lane = tid % G;
     const long long e = (long long)blockIdx.x * EPC + le;
-    const bool valid = e < A.E;
+    const bool valid = element_enabled(A, e);
 
     for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
         (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
@@ -111,21 +111,23 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : 8) k_element(Ele
                                                    (unsigned long long)__float_as_uint((float)detF);
                     atomicMin(&A.status->negdet_first, key);
                     atomicAdd(&A.status->negdet_count, 1u);
-                    report_status(A.status, NB2_E_NEG_DETJ);
+                    report_status(A, e, NB2_E_NEG_DETJ);
                 }
+                // per-element moduli (batched instances, parameter fields) replace the material's
+                const ElementArgs Ae = element_moduli(A, e);
                 if constexpr (MODEL == MODEL_LE) {
-                    cm_linear_elastic(A, Hm, o);
+                    cm_linear_elastic(Ae, Hm, o);
                 } else if constexpr (MODEL == MODEL_NH) {
-                    cm_neo_hooke(A, Fd, detF, o);
+                    cm_neo_hooke(Ae, Fd, detF, o);
                 } else if constexpr (MODEL == MODEL_J2) {
-                    if (!cm_j2(A, q, Hm, o)) report_status(A.status, NB2_E_RETURN_MAP);
+                    if (!cm_j2(A, q, Hm, o)) report_status(A, e, NB2_E_RETURN_MAP);
                 } else {
-                    cm_microsphere(A, A.Ge ? A.Ge[e] : A.G, Fd, detF, o);
+                    cm_microsphere(Ae, Ae.G, Fd, detF, o);
                 }
                 bool bad = isnan(o.lam) || isnan(o.mu);
 #pragma unroll
                 for (int c = 0; c < 6; ++c) bad |= isnan(o.sig[c]);
-                if (bad) report_status(A.status, NB2_E_NAN);
+                if (bad) report_status(A, e, NB2_E_NAN);
                 if constexpr (kStore) {
                     const long long n = A.nqp;
 #pragma unroll

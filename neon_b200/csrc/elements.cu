@@ -245,8 +245,26 @@ __device__ __forceinline__ void cm_microsphere(const ElementArgs& A, double Gm, 
     o.b = 0.0;
 }
 
-__device__ __forceinline__ void report_status(DeviceStatus* st, int code) {
-    atomicOr(&st->flags, 1u << (code - 1));
+// The material moduli of element e: per-element shear / bulk modulus when given (batched
+// instances of different materials, per-element parameter fields), else the material's.
+__device__ __forceinline__ ElementArgs element_moduli(const ElementArgs& A, long long e) {
+    ElementArgs Ae = A;
+    if (A.Ge || A.Ke) {
+        if (A.Ge) Ae.G = A.Ge[e];
+        if (A.Ke) Ae.K = A.Ke[e];
+        Ae.lambda = Ae.K - 2.0 * Ae.G / 3.0;
+    }
+    return Ae;
+}
+
+__device__ __forceinline__ void report_status(const ElementArgs& A, long long e, int code) {
+    atomicOr(&A.status->flags, 1u << (code - 1));
+    if (A.inst_flags) atomicOr(&A.inst_flags[A.e_inst[e]], 1u << (code - 1));
+}
+
+// batched solves compute only the elements of the instances still iterating
+__device__ __forceinline__ bool element_enabled(const ElementArgs& A, long long e) {
+    return e < A.E && (A.inst_on == nullptr || A.inst_on[A.e_inst[e]] != 0);
 }
 
 #include "element_kernel.cuh"
@@ -273,7 +291,7 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
     const int le = tid / G;
     const int lane = tid % G;
     const long long e = (long long)blockIdx.x * EPC + le;
-    const bool valid = e < A.E;
+    const bool valid = element_enabled(A, e);
     for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
         (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
     int node[(NPE + G - 1) / G];
@@ -489,6 +507,219 @@ __global__ void __launch_bounds__(64) k_adjoint_shear(ElementArgs A, const doubl
 }
 
 // ---------------------------------------------------------------------------------------
+// Exact directional derivative of the internal force, y = (d f_int / d u) v, by forward-mode
+// differentiation (dual numbers) of the element force.  neon's assembled tangents are not the
+// exact derivative of its f_int (the Kirchhoff moduli enter without 1/J, and the microsphere
+// drops the -2/3 (dev tau (x) I + I (x) dev tau) term), so an adjoint that must match finite
+// differences of the forward solve uses this product for its defect residual.  Hyperelastic
+// and small-strain elastic models (no history): NH, microsphere, linear elasticity.
+// ---------------------------------------------------------------------------------------
+struct Dual {
+    double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+    return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)};
+}
+__device__ __forceinline__ Dual dlog(Dual a) { return {log(a.v), a.d / a.v}; }
+__device__ __forceinline__ Dual dpow(Dual a, double p) {
+    const double f = pow(a.v, p);
+    return {f, p * f / a.v * a.d};
+}
+__device__ __forceinline__ Dual ddet3(const Dual* m) {
+    return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+           m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+__device__ __forceinline__ void dinv3(const Dual* m, Dual* r) {
+    const Dual c00 = m[4] * m[8] - m[5] * m[7], c10 = m[7] * m[2] - m[8] * m[1],
+               c20 = m[1] * m[5] - m[2] * m[4];
+    const Dual det = c00 * m[0] + c10 * m[3] + c20 * m[6];
+    const Dual id = Dual{1.0, 0.0} / det;
+    r[0] = c00 * id;
+    r[1] = c10 * id;
+    r[2] = c20 * id;
+    r[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+    r[4] = (m[8] * m[0] - m[6] * m[2]) * id;
+    r[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    r[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+    r[7] = (m[6] * m[1] - m[7] * m[0]) * id;
+    r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+// Cauchy stress (11 22 33 23 13 12) of the path's stateless models as a function of F, H
+template <int MODEL>
+__device__ __forceinline__ void dual_stress(const ElementArgs& A, double Gm, const Dual* F,
+                                            const Dual* H, Dual* s) {
+    if constexpr (MODEL == MODEL_LE) {
+        const Dual e3 = 0.5 * (H[5] + H[7]), e4 = 0.5 * (H[2] + H[6]), e5 = 0.5 * (H[1] + H[3]);
+        const Dual tr = H[0] + H[4] + H[8];
+        s[0] = A.lambda * tr + 2.0 * A.G * H[0];
+        s[1] = A.lambda * tr + 2.0 * A.G * H[4];
+        s[2] = A.lambda * tr + 2.0 * A.G * H[8];
+        s[3] = 2.0 * A.G * e3;
+        s[4] = 2.0 * A.G * e4;
+        s[5] = 2.0 * A.G * e5;
+    } else if constexpr (MODEL == MODEL_NH) {
+        const Dual J = ddet3(F);
+        Dual B[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                B[i * 3 + j] = F[i * 3 + 0] * F[j * 3 + 0] + F[i * 3 + 1] * F[j * 3 + 1] +
+                               F[i * 3 + 2] * F[j * 3 + 2];
+        const Dual lnJ = dlog(J);
+        const double mu = A.G, lam = A.lambda;
+        const Dual one{1.0, 0.0};
+        s[0] = (lam * lnJ + mu * (B[0] - one)) / J;
+        s[1] = (lam * lnJ + mu * (B[4] - one)) / J;
+        s[2] = (lam * lnJ + mu * (B[8] - one)) / J;
+        s[3] = (mu * B[5]) / J;
+        s[4] = (mu * B[2]) / J;
+        s[5] = (mu * B[1]) / J;
+    } else {
+        const double K = A.K;
+        const Dual J = ddet3(F);
+        const Dual sc = dpow(J, -1.0 / 3.0);
+        Dual acc[6] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}};
+        for (int i = 0; i < 21; ++i) {
+            const double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1],
+                         r2 = c_sphere_r[3 * i + 2], w = c_sphere_w[i];
+            const Dual t0 = sc * (r0 * F[0] + r1 * F[1] + r2 * F[2]);
+            const Dual t1 = sc * (r0 * F[3] + r1 * F[4] + r2 * F[5]);
+            const Dual t2 = sc * (r0 * F[6] + r1 * F[7] + r2 * F[8]);
+            acc[0] = acc[0] + w * (t0 * t0);
+            acc[1] = acc[1] + w * (t1 * t1);
+            acc[2] = acc[2] + w * (t2 * t2);
+            acc[3] = acc[3] + w * (t1 * t2);
+            acc[4] = acc[4] + w * (t0 * t2);
+            acc[5] = acc[5] + w * (t0 * t1);
+        }
+        Dual tau[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) tau[c] = (3.0 * Gm) * acc[c];
+        const Dual invJ = Dual{1.0, 0.0} / J;
+        const Dual p = J * ((K / 2.0) * (J - invJ));
+        const Dual tr3 = (1.0 / 3.0) * (tau[0] + tau[1] + tau[2]);
+        s[0] = (p + tau[0] - tr3) / J;
+        s[1] = (p + tau[1] - tr3) / J;
+        s[2] = (p + tau[2] - tr3) / J;
+        s[3] = tau[3] / J;
+        s[4] = tau[4] / J;
+        s[5] = tau[5] / J;
+    }
+}
+
+template <int NPE, int MODEL>
+__global__ void __launch_bounds__(64) k_force_jvp(ElementArgs A, const double* __restrict__ v,
+                                                  double* __restrict__ y) {
+    using T = Topo<NPE>;
+    constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC;
+    __shared__ double sX[EPC][NPE][3];
+    __shared__ double sx[EPC][NPE][3];
+    __shared__ double sv[EPC][NPE][3];
+    __shared__ double sdN[NQ][NPE][3];
+    const int tid = threadIdx.x;
+    const int le = tid / G;
+    const int lane = tid % G;
+    const long long e = (long long)blockIdx.x * EPC + le;
+    const bool valid = e < A.E;
+    for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
+        (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
+    int node[(NPE + G - 1) / G];
+#pragma unroll
+    for (int j = 0; j < (NPE + G - 1) / G; ++j) {
+        const int a = lane + j * G;
+        node[j] = 0;
+        if (a < NPE && valid) {
+            const int nd = A.conn[e * NPE + a];
+            node[j] = nd;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double Xv = A.X[3ll * nd + k];
+                sX[le][a][k] = Xv;
+                sx[le][a][k] = A.u[3ll * nd + k] + Xv;
+                sv[le][a][k] = v[3ll * nd + k];
+            }
+        }
+    }
+    __syncthreads();
+    const int l = lane;
+    const bool active = valid && l < NQ;
+    Dual Ji[9], s{0.0, 0.0}, sig[6];
+    if (active) {
+        const double w = (NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0);
+        Dual Fc[9], U[9];
+        double F0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Fc[i] = U[i] = Dual{0.0, 0.0};
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const Dual xi{sx[le][a][i], sv[le][a][i]};
+                const Dual di{sx[le][a][i] - sX[le][a][i], sv[le][a][i]};
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const double d = sdN[l][a][k];
+                    Fc[i * 3 + k] = Fc[i * 3 + k] + d * xi;
+                    U[i * 3 + k] = U[i * 3 + k] + d * di;
+                    F0[i * 3 + k] += sX[le][a][i] * d;
+                }
+            }
+        double F0i[9];
+        inv3(F0, F0i);
+        Dual Fd[9], Hm[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                Fd[i * 3 + j] = F0i[0 * 3 + j] * Fc[i * 3 + 0] + F0i[1 * 3 + j] * Fc[i * 3 + 1] +
+                                F0i[2 * 3 + j] * Fc[i * 3 + 2];
+                Hm[i * 3 + j] = F0i[0 * 3 + j] * U[i * 3 + 0] + F0i[1 * 3 + j] * U[i * 3 + 1] +
+                                F0i[2 * 3 + j] * U[i * 3 + 2];
+            }
+        const ElementArgs Ae = element_moduli(A, e);
+        dual_stress<MODEL>(Ae, Ae.G, Fd, Hm, sig);
+        dinv3(Fc, Ji);
+        s = w * ddet3(Fc);
+    }
+    double fown[(NPE + G - 1) / G][3];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+        double g[3] = {0.0, 0.0, 0.0};
+        if (active) {
+            Dual La[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                La[k] = sdN[l][a][0] * Ji[0 * 3 + k] + sdN[l][a][1] * Ji[1 * 3 + k] +
+                        sdN[l][a][2] * Ji[2 * 3 + k];
+            g[0] = (s * (sig[0] * La[0] + sig[5] * La[1] + sig[4] * La[2])).d;
+            g[1] = (s * (sig[5] * La[0] + sig[1] * La[1] + sig[3] * La[2])).d;
+            g[2] = (s * (sig[4] * La[0] + sig[3] * La[1] + sig[2] * La[2])).d;
+        }
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) g[k] += __shfl_xor_sync(0xffffffffu, g[k], off);
+        if (a % G == lane)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) fown[a / G][k] = g[k];
+    }
+    if (!valid) return;
+#pragma unroll
+    for (int j = 0; j < (NPE + G - 1) / G; ++j) {
+        const int a = lane + j * G;
+        if (a < NPE)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) atomicAdd(&y[3ll * node[j] + k], fown[j][k]);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
 static bool g_tables_ready = false;
@@ -590,13 +821,40 @@ static void launch_apply_t(nb2_ctx* c, const ElementArgs& A, const double* v, do
 int launch_apply(nb2_ctx* c, const double* v, double* y) {
     int st = upload_tables(c);
     if (st) return st;
-    if (!c->dpar) return NB2_E_INPUT;
+    if (!c->dpar || !c->u_tan) return NB2_E_INPUT;
     ElementArgs A = make_args(c);
+    A.u = c->u_tan;
     NB2_CUDA(c, cudaMemsetAsync(y, 0, sizeof(double) * c->n, c->stream));
     if (c->npe == 8)
         launch_apply_t<8>(c, A, v, y);
     else
         launch_apply_t<4>(c, A, v, y);
+    NB2_CUDA(c, cudaGetLastError());
+    return NB2_OK;
+}
+
+template <int NPE>
+static int launch_jvp_t(nb2_ctx* c, const ElementArgs& A, const double* v, double* y) {
+    constexpr int EPC = Topo<NPE>::EPC, G = Topo<NPE>::G;
+    const unsigned grid = (unsigned)((c->E + EPC - 1) / EPC);
+    switch (c->mat.model) {
+        case MODEL_LE: k_force_jvp<NPE, MODEL_LE><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+        case MODEL_NH: k_force_jvp<NPE, MODEL_NH><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+        case MODEL_MS: k_force_jvp<NPE, MODEL_MS><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+        default: return NB2_E_INPUT;  // J2 carries history: no exact tangent product here
+    }
+    c->launches++;
+    return NB2_OK;
+}
+
+// y = (d f_int / d u) v exactly (forward-mode), at the context displacement
+int launch_force_jvp(nb2_ctx* c, const double* v, double* y) {
+    int st = upload_tables(c);
+    if (st) return st;
+    ElementArgs A = make_args(c);
+    NB2_CUDA(c, cudaMemsetAsync(y, 0, sizeof(double) * c->n, c->stream));
+    st = c->npe == 8 ? launch_jvp_t<8>(c, A, v, y) : launch_jvp_t<4>(c, A, v, y);
+    if (st) return st;
     NB2_CUDA(c, cudaGetLastError());
     return NB2_OK;
 }
@@ -631,6 +889,7 @@ static ElementArgs make_args(nb2_ctx* c) {
     A.sigma_y = c->mat.yield_stress;
     A.H_iso = c->mat.isotropic_hardening_modulus;
     A.Ge = c->Ge;
+    A.Ke = c->Ke;
     A.ep = c->ep;
     A.epbar = c->epbar;
     A.K64 = c->K64;
@@ -640,34 +899,16 @@ static ElementArgs make_args(nb2_ctx* c) {
     A.dpar = c->dpar;
     A.detF = c->detF;
     A.status = c->status;
+    A.e_inst = c->e_inst;
+    A.inst_on = c->inst_on;
+    A.inst_flags = c->inst_flags;
     return A;
 }
 
 int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
     int st = upload_tables(c);
     if (st) return st;
-    ElementArgs A;
-    A.X = c->X;
-    A.u = c->u;
-    A.conn = c->conn;
-    A.slot = c->slot;
-    A.E = c->E;
-    A.nqp = c->nqp;
-    A.K = c->mat.bulk_modulus;
-    A.G = c->mat.shear_modulus;
-    A.lambda = c->mat.bulk_modulus - 2.0 * c->mat.shear_modulus / 3.0;
-    A.sigma_y = c->mat.yield_stress;
-    A.H_iso = c->mat.isotropic_hardening_modulus;
-    A.Ge = c->Ge;
-    A.ep = c->ep;
-    A.epbar = c->epbar;
-    A.K64 = c->K64;
-    A.K32 = c->K32;
-    A.fint = c->fint;
-    A.sig = c->sig;
-    A.dpar = c->dpar;
-    A.detF = c->detF;
-    A.status = c->status;
+    const ElementArgs A = make_args(c);
     if (mode & MODE_STIFFNESS) {
         if (precision == NB2_FP64)
             NB2_CUDA(c, cudaMemsetAsync(c->K64, 0, sizeof(double) * 9 * c->nnzb, c->stream));
@@ -678,6 +919,11 @@ int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
     st = (c->npe == 8) ? dispatch_model<8>(c, A, mode, precision)
                        : dispatch_model<4>(c, A, mode, precision);
     if (st) return st;
+    // the matrix-free tangent re-derives the gradients from this displacement, not from a
+    // later one (the Newton step adds the prescribed increment before its first solve)
+    if ((mode & MODE_STORE) && c->u_tan)
+        NB2_CUDA(c, cudaMemcpyAsync(c->u_tan, c->u, sizeof(double) * c->n,
+                                    cudaMemcpyDeviceToDevice, c->stream));
     NB2_CUDA(c, cudaGetLastError());
     return NB2_OK;
 }

@@ -47,7 +47,8 @@ struct ElementArgs {
     int E;
     int nqp;
     double K, G, lambda, sigma_y, H_iso;
-    const double* Ge;
+    const double* Ge;  // per-element shear modulus (or null)
+    const double* Ke;  // per-element bulk modulus (or null)
     double* ep;      // [6][nqp]
     double* epbar;   // [nqp]
     double* K64;     // [nnzb][9]
@@ -57,6 +58,11 @@ struct ElementArgs {
     double* dpar;    // [9][nqp]
     double* detF;    // [nqp]
     DeviceStatus* status;
+    // batched instances (all null outside a batched solve): element -> instance, the instances
+    // whose elements this pass computes, per-instance status flags
+    const int* e_inst;
+    const int* inst_on;
+    unsigned int* inst_flags;
 };
 
 // PCG scalars kept on the device (no host round trip per iteration)
@@ -101,6 +107,7 @@ struct nb2_ctx {
     double* inc = nullptr;  // prescribed increment
     unsigned char* mask = nullptr;  // active Dirichlet DOFs
     double* Ge = nullptr;
+    double* Ke = nullptr;
 
     // quadrature-point state
     double* ep = nullptr;
@@ -110,6 +117,7 @@ struct nb2_ctx {
     double* sig = nullptr;
     double* dpar = nullptr;
     double* detF = nullptr;
+    double* u_tan = nullptr;  // displacement of the last MODE_STORE pass (its geometry)
 
     // PCG workspace (FP64 and FP32 views share nothing)
     double *cg_x = nullptr, *cg_r = nullptr, *cg_p = nullptr, *cg_q = nullptr, *cg_inv = nullptr;
@@ -123,6 +131,12 @@ struct nb2_ctx {
     nb2::DeviceStatus* status = nullptr;
 
     cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;  // captured CG iteration blocks
+
+    // batched solves: set for the duration of one (device arrays owned by the batch state)
+    const int* e_inst = nullptr;
+    const int* inst_on = nullptr;
+    unsigned int* inst_flags = nullptr;
+    int batch_rows = 0, batch_lanes = 0;  // autotuned chunk rows / lanes per block row (0: default)
 
     long long launches = 0;
     std::string error;
@@ -142,6 +156,19 @@ int cuda_fail(nb2_ctx* c, cudaError_t e, const char* what);
         if (_e != cudaSuccess) return nb2::cuda_fail(ctx, _e, #call); \
     } while (0)
 
+#define NB2_TRY(x)                   \
+    do {                             \
+        int _s = (x);                \
+        if (_s != NB2_OK) return _s; \
+    } while (0)
+
+// api.cu: lazily allocated buffers and the element status word
+int ensure_k64(nb2_ctx* c);            // K64
+int ensure_k32(nb2_ctx* c);            // K32 and the FP32 CG vectors
+int ensure_split_buffers(nb2_ctx* c);  // stored quadrature-point outputs + their displacement
+int reset_status(nb2_ctx* c);
+int read_status(nb2_ctx* c);           // synchronises; the status code + neon's message
+
 // pattern.cu
 int build_pattern(nb2_ctx* c);
 int export_csr_values(nb2_ctx* c, const double* Kbsr, double* Kcsr_dev);
@@ -150,6 +177,7 @@ int export_csr_values(nb2_ctx* c, const double* Kbsr, double* Kcsr_dev);
 int launch_element_kernel(nb2_ctx* c, int mode, int precision);
 int launch_apply(nb2_ctx* c, const double* v, double* y);  // y = K v, FP64 matrix-free
 int launch_adjoint_shear(nb2_ctx* c, const double* lam, double* dJdG);
+int launch_force_jvp(nb2_ctx* c, const double* v, double* y);  // exact (d f_int/du) v
 void element_flop_model(const nb2_ctx* c, double* flops_per_element);
 
 // pcg.cu

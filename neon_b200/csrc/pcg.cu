@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(kRedThreads) k_spmv_bulk(Bsr<V> A, BulkPlan pl
     extern __shared__ __align__(128) unsigned char dyn[];
     __shared__ unsigned long long bar[kStages];
     __shared__ int timed_out;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned char* stage_base[kStages];
 #pragma unroll
     for (int i = 0; i < kStages; ++i)
@@ -531,9 +531,11 @@ __global__ void k_invdiag(Bsr<V> A, X* __restrict__ inv) {
         else
             hi = mid;
     }
+    // a node that no element references has an empty row: its diagonal is 0 (inverse 1)
+    const bool has = lo < A.brp[a + 1] && A.bcol[lo] == a;
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-        V d = A.val[9ll * lo + 4 * r];
+        V d = has ? A.val[9ll * lo + 4 * r] : (V)0;
         inv[3ll * a + r] = (d != (V)0) ? (X)(1.0 / (double)d) : (X)1;
     }
 }
