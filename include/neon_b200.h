@@ -180,6 +180,10 @@ int nb2_assemble(nb2_ctx* ctx, double* K_values, double* f_int);
  * nb2_update_internal_variables -- the same K nb2_assemble returns, applied element by element
  * without forming it (the defect residual of the mixed-precision solve). */
 int nb2_apply_tangent(nb2_ctx* ctx, const double* v, double* y);
+/* The same product with the FP32 matrix-free operator the mixed-precision PCG iterates with
+ * (FP32 relative coordinates and tangent coefficients per quadrature point, node-ordered sums;
+ * FP64 in and out).  Equals nb2_apply_tangent to FP32 rounding.  No reference counterpart. */
+int nb2_apply_tangent_fp32(nb2_ctx* ctx, const double* v, double* y);
 
 /* submesh::save_internal_variables (submesh.cpp:54-64): commit (1) or revert (0). */
 int nb2_save_internal_variables(nb2_ctx* ctx, int32_t converged);

@@ -100,6 +100,7 @@ _SIGS = {
     "nb2_assemble": (C.c_int, [P, P, P]),
     "nb2_save_internal_variables": (C.c_int, [P, C.c_int32]),
     "nb2_apply_tangent": (C.c_int, [P, P, P]),
+    "nb2_apply_tangent_fp32": (C.c_int, [P, P, P]),
     "nb2_get_quadrature_values": (C.c_int, [P, C.c_int32, P]),
     "nb2_apply_dirichlet": (C.c_int, [P, P, C.c_int32, P, P]),
     "nb2_pcg_solve": (C.c_int, [C.c_int32, P, P, P, P, P, C.c_double, C.c_int32,
@@ -228,6 +229,14 @@ class SolidMesh:
         v = np.ascontiguousarray(v, dtype=np.float64)
         y = np.zeros(self.ndofs)
         _check(lib().nb2_apply_tangent(self.h, v.ctypes.data, y.ctypes.data), self.h, "apply")
+        return y
+
+    def apply_tangent_fp32(self, v):
+        """K v with the FP32 matrix-free operator of the mixed-precision PCG."""
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        y = np.zeros(self.ndofs)
+        _check(lib().nb2_apply_tangent_fp32(self.h, v.ctypes.data, y.ctypes.data), self.h,
+               "apply_tangent_fp32")
         return y
 
     def save_internal_variables(self, converged: bool):

@@ -218,7 +218,7 @@ int nb2_destroy(nb2_ctx* c) {
     void* ptrs[] = {c->X,      c->conn,   c->brp,    c->bcol,   c->slot,      c->K64,
                     c->K32,    c->u,      c->u_old,  c->fint,   c->fext,      c->rhs,
                     c->du,     c->inc,    c->mask,   c->Ge,     c->Ke,        c->ep,
-                    c->epbar,  c->u_tan,
+                    c->epbar,  c->u_tan, c->mf_d, c->mf_c, c->mf_ye, c->nadj, c->nadj_ptr,
                     c->ep_old, c->epbar_old, c->sig, c->dpar,   c->detF,      c->cg_x,
                     c->cg_r,   c->cg_p,   c->cg_q,   c->cg_inv, c->cg32_x,    c->cg32_r,
                     c->cg32_p, c->cg32_q, c->cg32_inv, c->partials, c->cgs,   c->norms,
@@ -481,6 +481,26 @@ int nb2_synchronize(nb2_ctx* c) {
     return NB2_OK;
 }
 
+int nb2_apply_tangent_fp32(nb2_ctx* c, const double* v, double* y) {
+    if (!c || !v || !y) return NB2_E_INPUT;
+    if (!c->dpar) {
+        c->error = "nb2_apply_tangent_fp32 needs a prior nb2_update_internal_variables";
+        return NB2_E_INPUT;
+    }
+    double *dv = nullptr, *dy = nullptr;
+    NB2_CUDA(c, cudaMallocAsync(&dv, sizeof(double) * c->n, c->stream));
+    NB2_CUDA(c, cudaMallocAsync(&dy, sizeof(double) * c->n, c->stream));
+    NB2_CUDA(c, cudaMemcpyAsync(dv, v, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->stream));
+    int st = mf_apply(c, dv, dy);
+    if (st == NB2_OK)
+        NB2_CUDA(c, cudaMemcpyAsync(y, dy, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
+                                    c->stream));
+    cudaFreeAsync(dv, c->stream);
+    cudaFreeAsync(dy, c->stream);
+    NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    return st;
+}
+
 int nb2_apply_tangent(nb2_ctx* c, const double* v, double* y) {
     if (!c || !v || !y) return NB2_E_INPUT;
     if (!c->dpar) {
@@ -543,13 +563,14 @@ int nb2_solve_device(nb2_ctx* c, int32_t precision, double tol, int32_t maxit, i
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------------
-// Mixed-precision solve of K out = rhs (masked rows): FP64 defect correction around FP32 inner
-// PCG solves on K32; the defect rhs - K out applies the FP64 tangent matrix-free (the
-// coefficients stored by the last MODE_STORE element pass), so out converges to the solution of
-// the FP64 system to the relative tolerance `tol`.  rlin, corr, yvec: n-vector work space.
+// Defect correction for K_outer out = rhs (masked rows): restarted inner PCG solves on an
+// approximate operator (inner: NB2_MIXED = FP32 K32, NB2_FP64 = K64) to the relative tolerance
+// inner_tol, each correcting the residual rhs - K_outer out formed in FP64 with K_outer = the
+// stored tangent applied matrix-free, or (exact) the forward-mode product (d f_int/du) v.  out
+// converges to the solution of the outer system to the relative tolerance `tol`.  rlin, corr,
+// yvec: n-vector work space.  The Newton path's mixed solve (same operator inside and out) uses
+// the reliable-update PCG instead, which keeps its Krylov space across residual replacements.
 // ---------------------------------------------------------------------------------------
-// inner: NB2_MIXED (FP32 K32 inner PCG) or NB2_FP64 (K64); exact: the defect uses the exact
-// forward-mode product (d f_int/du) v instead of the stored (assembled) tangent.
 static int solve_defect_corrected(nb2_ctx* c, const double* rhs, double* out, double tol,
                                   double inner_tol, int maxit, bool graphs, double* rlin,
                                   double* corr, double* yvec, int* iterations, int inner,
@@ -558,8 +579,10 @@ static int solve_defect_corrected(nb2_ctx* c, const double* rhs, double* out, do
 static int solve_mixed_system(nb2_ctx* c, const double* rhs, double* out, double tol,
                               double inner_tol, int maxit, bool graphs, double* rlin,
                               double* corr, double* yvec, int* iterations) {
-    return solve_defect_corrected(c, rhs, out, tol, inner_tol, maxit, graphs, rlin, corr, yvec,
-                                  iterations, NB2_MIXED, false);
+    (void)rlin;
+    (void)corr;
+    return pcg_reliable_mixed(c, rhs, out, tol, inner_tol, maxit, yvec, iterations, graphs,
+                              true);
 }
 
 static int solve_defect_corrected(nb2_ctx* c, const double* rhs, double* out, double tol,
@@ -747,9 +770,11 @@ struct Newton {
     int element_pass(bool assemble) {
         NB2_TRY(reset_status(c));
         time_begin();
-        int mode = MODE_CONSTITUTIVE | MODE_FORCE | (assemble ? MODE_STIFFNESS : 0);
-        if (mixed() && assemble) mode |= MODE_STORE;
-        NB2_TRY(launch_element_kernel(c, mode, mixed() ? NB2_MIXED : NB2_FP64));
+        // mixed: no assembled K at all -- the stored FP64 tangent feeds the lifting, the FP64
+        // residual replacements and the FP32 matrix-free operator of the PCG
+        int mode = MODE_CONSTITUTIVE | MODE_FORCE;
+        if (assemble) mode |= mixed() ? MODE_STORE : MODE_STIFFNESS;
+        NB2_TRY(launch_element_kernel(c, mode, NB2_FP64));
         t_elem += time_end();
         return read_status(c);
     }

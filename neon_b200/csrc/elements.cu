@@ -39,6 +39,8 @@ namespace nb2 {
 __constant__ double c_dN_hex8[8 * 8 * 3];
 __constant__ double c_w_hex8[8];
 __constant__ double c_dN_tet4[4 * 3];
+__constant__ float c_dNf_hex8[8 * 8 * 3];  // FP32 copies for the matrix-free FP32 operator
+__constant__ float c_dNf_tet4[4 * 3];
 __constant__ double c_sphere_r[21 * 3];
 __constant__ double c_sphere_w[21];
 
@@ -404,6 +406,8 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
     }
 }
 
+#include "mf_kernels.cuh"
+
 // ---------------------------------------------------------------------------------------
 // Adjoint gradient with respect to the per-element shear modulus of the Gaussian affine
 // microsphere.  With K lambda = dJ/du solved on the converged tangent,
@@ -760,6 +764,11 @@ static int upload_tables(nb2_ctx* c) {
     NB2_CUDA(c, cudaMemcpyToSymbol(c_dN_tet4, dNt, sizeof dNt));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_sphere_r, r, sizeof r));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_sphere_w, sw, sizeof sw));
+    float dNf[8 * 8 * 3], dNtf[12];
+    for (int i = 0; i < 8 * 8 * 3; ++i) dNf[i] = (float)dN[i];
+    for (int i = 0; i < 12; ++i) dNtf[i] = (float)dNt[i];
+    NB2_CUDA(c, cudaMemcpyToSymbol(c_dNf_hex8, dNf, sizeof dNf));
+    NB2_CUDA(c, cudaMemcpyToSymbol(c_dNf_tet4, dNtf, sizeof dNtf));
     g_tables_ready = true;
     return NB2_OK;
 }
@@ -831,6 +840,60 @@ int launch_apply(nb2_ctx* c, const double* v, double* y) {
         launch_apply_t<4>(c, A, v, y);
     NB2_CUDA(c, cudaGetLastError());
     return NB2_OK;
+}
+
+template <int NPE, int MODEL>
+static void mf_setup_t(nb2_ctx* c, const ElementArgs& A) {
+    constexpr int EPC = Topo<NPE>::EPC, G = Topo<NPE>::G;
+    const unsigned grid = (unsigned)((c->E + EPC - 1) / EPC);
+    k_mf_setup<NPE, MODEL><<<grid, EPC * G, 0, c->stream>>>(A, c->mf_d, c->mf_c, c->mf_ye);
+    c->launches++;
+}
+
+// FP32 matrix-free data of the tangent stored by the last MODE_STORE pass; the element
+// contributions to diag(K) are left in mf_ye for the gather that forms the Jacobi inverse
+int launch_mf_setup(nb2_ctx* c) {
+    int st = upload_tables(c);
+    if (st) return st;
+    if (!c->dpar || !c->u_tan || !c->mf_d) return NB2_E_INPUT;
+    ElementArgs A = make_args(c);
+    A.u = c->u_tan;
+    const bool hex = c->npe == 8;
+    switch (c->mat.model) {
+        case MODEL_LE: hex ? mf_setup_t<8, MODEL_LE>(c, A) : mf_setup_t<4, MODEL_LE>(c, A); break;
+        case MODEL_NH: hex ? mf_setup_t<8, MODEL_NH>(c, A) : mf_setup_t<4, MODEL_NH>(c, A); break;
+        case MODEL_J2: hex ? mf_setup_t<8, MODEL_J2>(c, A) : mf_setup_t<4, MODEL_J2>(c, A); break;
+        default: hex ? mf_setup_t<8, MODEL_MS>(c, A) : mf_setup_t<4, MODEL_MS>(c, A); break;
+    }
+    NB2_CUDA(c, cudaGetLastError());
+    return NB2_OK;
+}
+
+int mf_coefficients(int model) {
+    switch (model) {
+        case MODEL_LE: return MfCoef<MODEL_LE>::KC;
+        case MODEL_NH: return MfCoef<MODEL_NH>::KC;
+        case MODEL_J2: return MfCoef<MODEL_J2>::KC;
+        default: return MfCoef<MODEL_MS>::KC;
+    }
+}
+
+template <int NPE, int MODEL>
+static void apply32_t(nb2_ctx* c, const float* v, float* ye, const int* done) {
+    const unsigned grid = (unsigned)((c->E + kApply32Threads - 1) / kApply32Threads);
+    k_apply32<NPE, MODEL><<<grid, kApply32Threads, 0, c->stream>>>(c->E, c->conn, c->mf_d, c->mf_c,
+                                                                   c->nqp, v, ye, done);
+}
+
+// ye = K_e v_e per element in FP32 (graph-capturable: launches only)
+void enqueue_apply32(nb2_ctx* c, const float* v, float* ye, const int* done) {
+    const bool hex = c->npe == 8;
+    switch (c->mat.model) {
+        case MODEL_LE: hex ? apply32_t<8, MODEL_LE>(c, v, ye, done) : apply32_t<4, MODEL_LE>(c, v, ye, done); break;
+        case MODEL_NH: hex ? apply32_t<8, MODEL_NH>(c, v, ye, done) : apply32_t<4, MODEL_NH>(c, v, ye, done); break;
+        case MODEL_J2: hex ? apply32_t<8, MODEL_J2>(c, v, ye, done) : apply32_t<4, MODEL_J2>(c, v, ye, done); break;
+        default: hex ? apply32_t<8, MODEL_MS>(c, v, ye, done) : apply32_t<4, MODEL_MS>(c, v, ye, done); break;
+    }
 }
 
 template <int NPE>

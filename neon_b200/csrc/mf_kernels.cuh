@@ -1,0 +1,298 @@
+// mf_kernels.cuh -- the FP32 matrix-free tangent product of the mixed-precision PCG (included
+// by elements.cu, which owns the shape-function tables).
+//
+// The assembled FP32 K of a hex8 mesh costs ~27 blocks x 40 B = 1.1 KB per element per SpMV.
+// The same operator applied element by element needs far less: per element the FP32 node
+// coordinates relative to its first node (96 B; differences taken in FP64, so no cancellation
+// in FP32), per quadrature point the tangent coefficients pre-multiplied by w det J (2 floats;
+// J2 plastic points 9, finite strain 8), the node indices, and the input/output vectors.
+//   k_mf_setup  once per linear solve (after an element pass that stored its outputs): writes
+//               those FP32 data and each element's contribution to diag(K) (Jacobi);
+//   k_apply32   per CG iteration: y_e = K_e v_e in FP32, written per element (ye[E][npe*3]);
+//               a node-ordered gather (pcg.cu) sums ye into q without atomics, in a fixed order.
+// With G = sum_b v_b (x) L_b the element force of node a is (the product the assembled blocks
+//   K_ab = s[lam' La(x)Lb + mu'((La.Lb) I + Lb(x)La) + b (N La)(x)(N Lb)] + s (La.sigma.Lb) I
+// give) y_a = s [lam' tr(G) La + mu' (G + G^T) La + b (N:G) N La + G sigma La].
+#pragma once
+
+__device__ __forceinline__ float det3f(const float* m) {
+    return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+           m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+__device__ __forceinline__ void inv3f(const float* m, float* r) {
+    const float c00 = m[4] * m[8] - m[5] * m[7];
+    const float c10 = m[7] * m[2] - m[8] * m[1];
+    const float c20 = m[1] * m[5] - m[2] * m[4];
+    const float id = 1.0f / (c00 * m[0] + c10 * m[3] + c20 * m[6]);
+    r[0] = c00 * id;
+    r[1] = c10 * id;
+    r[2] = c20 * id;
+    r[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+    r[4] = (m[8] * m[0] - m[6] * m[2]) * id;
+    r[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    r[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+    r[7] = (m[6] * m[1] - m[7] * m[0]) * id;
+    r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+// number of FP32 coefficients per quadrature point
+template <int MODEL>
+struct MfCoef {
+    static constexpr int KC = (MODEL == MODEL_J2) ? 9 : ((MODEL == MODEL_LE) ? 2 : 8);
+};
+
+// Setup from the stored FP64 outputs of the last MODE_STORE pass (A.u = its displacement):
+//   md[e][3a+k]  = (float)(x_a - x_0)_k
+//   mc[c][q]     = s lam', s mu' | J2: s b, N (6) | finite strain: s sigma (6)
+//   de[e][3a+i]  = element contribution to K_(3a+i, 3a+i)
+template <int NPE, int MODEL>
+__global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restrict__ md,
+                                                 float* __restrict__ mc, float* __restrict__ de) {
+    using T = Topo<NPE>;
+    constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC;
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
+    constexpr bool kJ2 = (MODEL == MODEL_J2);
+    __shared__ double sx[EPC][NPE][3];
+    __shared__ double sdN[NQ][NPE][3];
+    __shared__ double sD[EPC][NQ][NPE * 3];
+    const int tid = threadIdx.x;
+    const int le = tid / G;
+    const int lane = tid % G;
+    const long long e = (long long)blockIdx.x * EPC + le;
+    const bool valid = element_enabled(A, e);
+    for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
+        (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
+#pragma unroll
+    for (int j = 0; j < (NPE + G - 1) / G; ++j) {
+        const int a = lane + j * G;
+        if (a < NPE && valid) {
+            const int nd = A.conn[e * NPE + a];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) sx[le][a][k] = A.u[3ll * nd + k] + A.X[3ll * nd + k];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < (NPE + G - 1) / G; ++j) {
+        const int a = lane + j * G;
+        if (a < NPE && valid)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                md[e * NPE * 3 + 3 * a + k] = (float)(sx[le][a][k] - sx[le][0][k]);
+    }
+    for (int l = lane; l < NQ; l += G) {
+        if (!valid) break;
+        const double w = (NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0);
+        const long long q = e * NQ + l;
+        const long long n = A.nqp;
+        double Fc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) Fc[i * 3 + k] += sx[le][a][i] * sdN[l][a][k];
+        double Ji[9];
+        inv3(Fc, Ji);
+        const double s = w * det3(Fc);
+        const double lam = A.dpar[0 * n + q], mu = A.dpar[1 * n + q];
+        double b = 0.0, N6[6] = {0, 0, 0, 0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0};
+        mc[0 * n + q] = (float)(s * lam);
+        mc[1 * n + q] = (float)(s * mu);
+        if constexpr (kJ2) {
+            b = A.dpar[2 * n + q];
+            mc[2 * n + q] = (float)(s * b);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                N6[c] = A.dpar[(3 + c) * n + q];
+                mc[(3 + c) * n + q] = (float)N6[c];
+            }
+        }
+        if constexpr (kFinite) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                sg[c] = A.sig[c * n + q];
+                mc[(2 + c) * n + q] = (float)(s * sg[c]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+            double La[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                La[k] = sdN[l][a][0] * Ji[0 * 3 + k] + sdN[l][a][1] * Ji[1 * 3 + k] +
+                        sdN[l][a][2] * Ji[2 * 3 + k];
+            const double LL = La[0] * La[0] + La[1] * La[1] + La[2] * La[2];
+            double nl[3] = {0, 0, 0};
+            if constexpr (kJ2) {
+                nl[0] = N6[0] * La[0] + N6[5] * La[1] + N6[4] * La[2];
+                nl[1] = N6[5] * La[0] + N6[1] * La[1] + N6[3] * La[2];
+                nl[2] = N6[4] * La[0] + N6[3] * La[1] + N6[2] * La[2];
+            }
+            double geo = 0.0;
+            if constexpr (kFinite)
+                geo = sg[0] * La[0] * La[0] + sg[1] * La[1] * La[1] + sg[2] * La[2] * La[2] +
+                      2.0 * (sg[3] * La[1] * La[2] + sg[4] * La[0] * La[2] + sg[5] * La[0] * La[1]);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                sD[le][l][3 * a + i] =
+                    s * (lam * La[i] * La[i] + mu * (LL + La[i] * La[i]) + b * nl[i] * nl[i] + geo);
+        }
+    }
+    __syncthreads();
+    if (!valid) return;
+#pragma unroll
+    for (int j = 0; j < (NPE + G - 1) / G; ++j) {
+        const int a = lane + j * G;
+        if (a < NPE)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                double t = 0.0;
+#pragma unroll
+                for (int l = 0; l < NQ; ++l) t += sD[le][l][3 * a + i];
+                de[e * NPE * 3 + 3 * a + i] = (float)t;
+            }
+    }
+}
+
+// ye[e] = K_e v_e in FP32 from the setup data; skipped once the CG scalars say done.
+// One thread per element: its relative coordinates, input values and output stay in registers
+// and the shape derivatives are constant-memory operands, so the hot loops are FFMA only.  Per
+// point, with D = sum_a d_a (x) dN_a (= J), Gx = sum_a v_a (x) dN_a:
+//   G = Gx J^-1,  S = s[lam' tr(G) I + mu' (G + G^T) + b (N:G) N + G sigma],  P = S J^-T,
+//   y_a += P dN_a                     (y_a = S L_a with L_a = J^-T dN_a, never formed)
+constexpr int kApply32Threads = 128;
+
+template <int NPE>
+__device__ __forceinline__ float dNf(int i) {
+    if constexpr (NPE == 8)
+        return c_dNf_hex8[i];
+    else
+        return c_dNf_tet4[i];
+}
+
+template <int NPE, int MODEL>
+__global__ void __launch_bounds__(kApply32Threads) k_apply32(int E, const int* __restrict__ conn,
+                                                             const float* __restrict__ md,
+                                                             const float* __restrict__ mc,
+                                                             long long nqp,
+                                                             const float* __restrict__ v,
+                                                             float* __restrict__ ye,
+                                                             const int* __restrict__ done) {
+    using T = Topo<NPE>;
+    constexpr int NQ = T::NQ;
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
+    constexpr bool kJ2 = (MODEL == MODEL_J2);
+    if (done && *done) return;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    float d[NPE][3], vv[NPE][3], y[NPE][3];
+    {
+        const float4* m4 = reinterpret_cast<const float4*>(md + e * NPE * 3);
+#pragma unroll
+        for (int j = 0; j < NPE * 3 / 4; ++j) {
+            const float4 t = m4[j];
+            (&d[0][0])[4 * j + 0] = t.x;
+            (&d[0][0])[4 * j + 1] = t.y;
+            (&d[0][0])[4 * j + 2] = t.z;
+            (&d[0][0])[4 * j + 3] = t.w;
+        }
+        const int4* c4 = reinterpret_cast<const int4*>(conn + e * NPE);
+#pragma unroll
+        for (int j = 0; j < NPE / 4; ++j) {
+            const int4 t = c4[j];
+            const int nd[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) vv[4 * j + b][k] = v[3ll * nd[b] + k];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) y[a][0] = y[a][1] = y[a][2] = 0.0f;
+#pragma unroll
+    for (int l = 0; l < NQ; ++l) {
+        const long long q = e * NQ + l;
+        float J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        float Gx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float g = dNf<NPE>((l * NPE + a) * 3 + k);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    J[i * 3 + k] += d[a][i] * g;
+                    Gx[i * 3 + k] += vv[a][i] * g;
+                }
+            }
+        float Ji[9];
+        inv3f(J, Ji);
+        float G[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                G[i * 3 + k] = Gx[i * 3 + 0] * Ji[0 * 3 + k] + Gx[i * 3 + 1] * Ji[1 * 3 + k] +
+                               Gx[i * 3 + 2] * Ji[2 * 3 + k];
+        const float cl = mc[0 * nqp + q], cm = mc[1 * nqp + q];
+        const float ltr = cl * (G[0] + G[4] + G[8]);
+        float S[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                S[i * 3 + k] = cm * (G[i * 3 + k] + G[k * 3 + i]) + (i == k ? ltr : 0.0f);
+        if constexpr (kJ2) {
+            const float cb = mc[2 * nqp + q];
+            if (cb != 0.0f) {
+                float N6[6];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) N6[c] = mc[(3 + c) * nqp + q];
+                const float bN = cb * (N6[0] * G[0] + N6[1] * G[4] + N6[2] * G[8] +
+                                       N6[3] * (G[5] + G[7]) + N6[4] * (G[2] + G[6]) +
+                                       N6[5] * (G[1] + G[3]));
+                // N symmetric (11 22 33 23 13 12)
+                S[0] += bN * N6[0]; S[4] += bN * N6[1]; S[8] += bN * N6[2];
+                S[5] += bN * N6[3]; S[7] += bN * N6[3];
+                S[2] += bN * N6[4]; S[6] += bN * N6[4];
+                S[1] += bN * N6[5]; S[3] += bN * N6[5];
+            }
+        }
+        if constexpr (kFinite) {
+            float sg[9];
+            sg[0] = mc[2 * nqp + q]; sg[4] = mc[3 * nqp + q]; sg[8] = mc[4 * nqp + q];
+            sg[5] = sg[7] = mc[5 * nqp + q];
+            sg[2] = sg[6] = mc[6 * nqp + q];
+            sg[1] = sg[3] = mc[7 * nqp + q];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    S[i * 3 + k] += G[i * 3 + 0] * sg[0 * 3 + k] + G[i * 3 + 1] * sg[1 * 3 + k] +
+                                    G[i * 3 + 2] * sg[2 * 3 + k];
+        }
+        // P = S J^-T: P[i][k] = sum_j S[i][j] Ji[k][j]
+        float Pm[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                Pm[i * 3 + k] = S[i * 3 + 0] * Ji[k * 3 + 0] + S[i * 3 + 1] * Ji[k * 3 + 1] +
+                                S[i * 3 + 2] * Ji[k * 3 + 2];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+            const float g0 = dNf<NPE>((l * NPE + a) * 3 + 0), g1 = dNf<NPE>((l * NPE + a) * 3 + 1),
+                        g2 = dNf<NPE>((l * NPE + a) * 3 + 2);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                y[a][i] += Pm[i * 3 + 0] * g0 + Pm[i * 3 + 1] * g1 + Pm[i * 3 + 2] * g2;
+        }
+    }
+    float4* o4 = reinterpret_cast<float4*>(ye + e * NPE * 3);
+#pragma unroll
+    for (int j = 0; j < NPE * 3 / 4; ++j)
+        o4[j] = make_float4((&y[0][0])[4 * j + 0], (&y[0][0])[4 * j + 1], (&y[0][0])[4 * j + 2],
+                            (&y[0][0])[4 * j + 3]);
+}

@@ -119,6 +119,15 @@ struct nb2_ctx {
     double* detF = nullptr;
     double* u_tan = nullptr;  // displacement of the last MODE_STORE pass (its geometry)
 
+    // FP32 matrix-free tangent (mixed-precision PCG): per-element relative coordinates, per-point
+    // coefficients, per-element products / diagonal contributions, node -> element-slot lists
+    float* mf_d = nullptr;   // [E][npe*3]
+    float* mf_c = nullptr;   // [kc][nqp]
+    float* mf_ye = nullptr;  // [E][npe*3]
+    int* nadj_ptr = nullptr; // [N+1]
+    int* nadj = nullptr;     // [E*npe] element slots e*npe + a, grouped by node
+    cudaGraphExec_t graph_mf = nullptr;
+
     // PCG workspace (FP64 and FP32 views share nothing)
     double *cg_x = nullptr, *cg_r = nullptr, *cg_p = nullptr, *cg_q = nullptr, *cg_inv = nullptr;
     float *cg32_x = nullptr, *cg32_r = nullptr, *cg32_p = nullptr, *cg32_q = nullptr,
@@ -171,6 +180,7 @@ int read_status(nb2_ctx* c);           // synchronises; the status code + neon's
 
 // pattern.cu
 int build_pattern(nb2_ctx* c);
+int build_node_adjacency(nb2_ctx* c);  // nadj_ptr / nadj
 int export_csr_values(nb2_ctx* c, const double* Kbsr, double* Kcsr_dev);
 
 // elements.cu
@@ -178,6 +188,9 @@ int launch_element_kernel(nb2_ctx* c, int mode, int precision);
 int launch_apply(nb2_ctx* c, const double* v, double* y);  // y = K v, FP64 matrix-free
 int launch_adjoint_shear(nb2_ctx* c, const double* lam, double* dJdG);
 int launch_force_jvp(nb2_ctx* c, const double* v, double* y);  // exact (d f_int/du) v
+int launch_mf_setup(nb2_ctx* c);  // FP32 matrix-free data + diagonal contributions
+int mf_coefficients(int model);   // FP32 coefficients per quadrature point
+void enqueue_apply32(nb2_ctx* c, const float* v, float* ye, const int* done);
 void element_flop_model(const nb2_ctx* c, double* flops_per_element);
 
 // pcg.cu
@@ -190,6 +203,13 @@ int pcg_device_fp64(nb2_ctx* c, const double* b, double* x, double tol, int maxi
                     int* iterations, double* error, bool use_graphs);
 int pcg_device_fp32(nb2_ctx* c, const double* b, double* x, double tol, int maxit, int* iterations,
                     double* error, bool use_graphs);
+// mixed precision with reliable updates: FP32 iterations on K32, FP64 true residual (matrix-free
+// stored tangent) every `delta` reduction; work: n doubles
+int pcg_reliable_mixed(nb2_ctx* c, const double* b, double* x, double tol, double delta,
+                       int maxit, double* work, int* iterations, bool use_graphs,
+                       bool matrix_free);
+int ensure_mf(nb2_ctx* c);  // FP32 matrix-free buffers + node adjacency
+int mf_apply(nb2_ctx* c, const double* v, double* y);  // FP32 matrix-free K v (device FP64)
 int pcg_csr_host(int n, const int* rowptr, const int* col, const double* val, const double* b,
                  double* x, double tol, int maxit, int* iterations, double* error,
                  std::string* err);

@@ -115,6 +115,45 @@ int build_pattern(nb2_ctx* c) {
     return NB2_OK;
 }
 
+__global__ void k_iota(long long n, int* v) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (int)i;
+}
+
+// first position of each node in the node-sorted slot list (sorted keys: binary search)
+__global__ void k_node_starts(const int* keys, long long m, int N, int* ptr) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a > N) return;
+    long long lo = 0, hi = m;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (keys[mid] < a) lo = mid + 1; else hi = mid;
+    }
+    ptr[a] = (int)lo;
+}
+
+// For every node the element slots e*npe + a that reference it, in ascending slot order (a
+// stable sort keeps it), so the matrix-free gather sums them in a fixed order.
+int build_node_adjacency(nb2_ctx* c) {
+    if (c->nadj) return NB2_OK;
+    const long long m = (long long)c->E * c->npe;
+    int* keys = nullptr;
+    NB2_CUDA(c, cudaMallocAsync(&keys, sizeof(int) * m, c->stream));
+    NB2_CUDA(c, cudaMalloc(&c->nadj, sizeof(int) * m));
+    NB2_CUDA(c, cudaMalloc(&c->nadj_ptr, sizeof(int) * (c->N + 1)));
+    NB2_CUDA(c, cudaMemcpyAsync(keys, c->conn, sizeof(int) * m, cudaMemcpyDeviceToDevice, c->stream));
+    const int T = 256;
+    k_iota<<<(unsigned)((m + T - 1) / T), T, 0, c->stream>>>(m, c->nadj);
+    auto pol = thrust::cuda::par.on(c->stream);
+    thrust::device_ptr<int> kp(keys), vp(c->nadj);
+    thrust::stable_sort_by_key(pol, kp, kp + m, vp);
+    k_node_starts<<<(c->N + 1 + T - 1) / T, T, 0, c->stream>>>(keys, m, c->N, c->nadj_ptr);
+    c->launches += 2;
+    NB2_CUDA(c, cudaFreeAsync(keys, c->stream));
+    NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    return NB2_OK;
+}
+
 int export_csr_values(nb2_ctx* c, const double* Kbsr, double* Kcsr_dev) {
     const int T = 256;
     k_bsr_to_csr<<<(c->N + T / 32 - 1) / (T / 32), T, 0, c->stream>>>(c->brp, c->N, Kbsr, Kcsr_dev);

@@ -639,6 +639,92 @@ __global__ void __launch_bounds__(kRedThreads) k_bsr_apply(Bsr<V> A, const doubl
 }
 
 // ---------------------------------------------------------------------------------------
+// matrix-free FP32 operator: node-ordered gather of the per-element products
+// ---------------------------------------------------------------------------------------
+// q = sum over the node's element slots of ye (masked rows 0), p.q -> alpha (as k_spmv)
+template <typename X>
+__global__ void __launch_bounds__(kRedThreads) k_mf_gather(int N, const int* __restrict__ nptr,
+                                                           const int* __restrict__ nadj,
+                                                           const float* __restrict__ ye,
+                                                           const X* __restrict__ p,
+                                                           X* __restrict__ q,
+                                                           const unsigned char* __restrict__ mask,
+                                                           CgScalars* s, double* partials) {
+    if (s->done) return;
+    double dot[1] = {0.0};
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < N; a += gridDim.x * blockDim.x) {
+        float y0 = 0.0f, y1 = 0.0f, y2 = 0.0f;
+        const int k1 = nptr[a + 1];
+#pragma unroll 4
+        for (int k = nptr[a]; k < k1; ++k) {
+            const long long j = 3ll * nadj[k];
+            y0 += ye[j];
+            y1 += ye[j + 1];
+            y2 += ye[j + 2];
+        }
+        const float y[3] = {y0, y1, y2};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const long long i = 3ll * a + c;
+            const X v = mask[i] ? (X)0 : (X)y[c];
+            q[i] = v;
+            dot[0] += (double)p[i] * (double)v;
+        }
+    }
+    if (block_partials<1>(dot, partials, &s->counter[0])) {
+        double tot[1];
+        final_sum<1>(partials, tot);
+        if (threadIdx.x == 0) {
+            s->pq = tot[0];
+            s->alpha = s->abs_new / tot[0];
+            if (!isfinite(s->alpha)) {
+                s->status = NB2_E_NAN;
+                s->done = 1;
+            }
+            s->counter[0] = 0;
+        }
+    }
+}
+
+// y = sum over the node's element slots of ye (no mask, no reduction)
+__global__ void k_mf_sum(int N, const int* __restrict__ nptr, const int* __restrict__ nadj,
+                         const float* __restrict__ ye, double* __restrict__ y) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= N) return;
+    float s[3] = {0.0f, 0.0f, 0.0f};
+    for (int k = nptr[a]; k < nptr[a + 1]; ++k) {
+        const long long j = 3ll * nadj[k];
+        s[0] += ye[j];
+        s[1] += ye[j + 1];
+        s[2] += ye[j + 2];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) y[3ll * a + c] = (double)s[c];
+}
+
+__global__ void k_to_float(long long n, const double* __restrict__ a, float* __restrict__ b) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// Jacobi inverse from the per-element diagonal contributions (1 for a zero diagonal)
+__global__ void k_mf_diag(int N, const int* __restrict__ nptr, const int* __restrict__ nadj,
+                          const float* __restrict__ de, float* __restrict__ inv) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= N) return;
+    double d[3] = {0.0, 0.0, 0.0};
+    for (int k = nptr[a]; k < nptr[a + 1]; ++k) {
+        const long long j = 3ll * nadj[k];
+        d[0] += de[j];
+        d[1] += de[j + 1];
+        d[2] += de[j + 2];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) inv[3ll * a + c] = d[c] != 0.0 ? (float)(1.0 / d[c]) : 1.0f;
+}
+
+// ---------------------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------------------
 static int wait_scalars(nb2_ctx* c) {
@@ -675,43 +761,65 @@ static bool make_bulk_plan(const nb2_ctx* c, int vsize, BulkPlan* plan) {
     return false;
 }
 
+// One Jacobi-PCG on a block matrix: the bulk SpMV plan, the captured block of kChunk iterations
+// and the host loop that launches blocks until the device scalars say done.
 template <typename V, typename X>
-static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv, const double* b,
-                      double* xout, double tol, int maxit, bool use_mask, int* iterations,
-                      double* error, bool use_graphs, cudaGraphExec_t* cache) {
-    const int RB = reduction_blocks(c);
-    Bsr<V> A{c->brp, c->bcol, vals, c->N};
+struct CgRunner {
+    nb2_ctx* c;
+    const V* vals;
+    X *x, *r, *p, *q, *inv;
+    bool use_mask, use_graphs;
+    cudaGraphExec_t* cache;
+    bool mf = false;  // FP32 matrix-free operator (V = X = float) instead of the assembled K
+    int RB = 0;
+    Bsr<V> A{};
     BulkPlan plan{};
-    const bool bulk = make_bulk_plan(c, (int)sizeof(V), &plan);
+    bool bulk = false;
     int bulk_grid = 0;
     size_t bulk_smem = 0;
-    const int rpw = bulk ? plan.rows_per_chunk / kBulkWarps : 0;
-    auto bulk_kernel = [&]() -> void (*)(Bsr<V>, BulkPlan, const X*, X*, const unsigned char*,
-                                         CgScalars*, double*) {
+    void (*bulk_kernel)(Bsr<V>, BulkPlan, const X*, X*, const unsigned char*, CgScalars*,
+                        double*) = nullptr;
+
+    int setup() {
+        RB = reduction_blocks(c);
+        if (mf) return NB2_OK;  // the Jacobi inverse comes from the matrix-free setup
+        A = Bsr<V>{c->brp, c->bcol, vals, c->N};
+        bulk = make_bulk_plan(c, (int)sizeof(V), &plan);
+        const int rpw = bulk ? plan.rows_per_chunk / kBulkWarps : 0;
         switch (rpw) {
-            case 8: return k_spmv_bulk<V, X, 8>;
-            case 4: return k_spmv_bulk<V, X, 4>;
-            case 2: return k_spmv_bulk<V, X, 2>;
-            default: return k_spmv_bulk<V, X, 1>;
+            case 8: bulk_kernel = k_spmv_bulk<V, X, 8>; break;
+            case 4: bulk_kernel = k_spmv_bulk<V, X, 4>; break;
+            case 2: bulk_kernel = k_spmv_bulk<V, X, 2>; break;
+            default: bulk_kernel = k_spmv_bulk<V, X, 1>; break;
         }
-    }();
-    if (bulk) {
-        bulk_smem = (size_t)kStages * (plan.stage_val_bytes + plan.stage_col_bytes);
-        NB2_CUDA(c, cudaFuncSetAttribute(bulk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)bulk_smem));
-        const int per_sm = std::max(1, (int)((220 * 1024) / (bulk_smem + 4096)));
-        bulk_grid = std::min(plan.chunks, 148 * per_sm);
+        if (bulk) {
+            bulk_smem = (size_t)kStages * (plan.stage_val_bytes + plan.stage_col_bytes);
+            NB2_CUDA(c, cudaFuncSetAttribute(bulk_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)bulk_smem));
+            const int per_sm = std::max(1, (int)((220 * 1024) / (bulk_smem + 4096)));
+            bulk_grid = std::min(plan.chunks, 148 * per_sm);
+        }
+        k_invdiag<V, X><<<(c->N + 255) / 256, 256, 0, c->stream>>>(A, inv);
+        c->launches++;
+        return NB2_OK;
     }
-    const long long n = c->n;
-    k_invdiag<V, X><<<(c->N + 255) / 256, 256, 0, c->stream>>>(A, inv);
-    k_init<X><<<RB, kRedThreads, 0, c->stream>>>(n, b, x, r, p, inv, c->cgs, c->partials, tol);
-    c->launches += 2;
-    // max_iterations is read by k_xr: set it with a tiny copy
-    NB2_CUDA(c, cudaMemcpyAsync(&c->cgs->max_iterations, &maxit, sizeof(int), cudaMemcpyHostToDevice,
-                                c->stream));
-    const unsigned char* mask = use_mask ? c->mask : nullptr;
-    auto enqueue = [&](int count) {
+
+    void enqueue(int count) {
+        const unsigned char* mask = use_mask ? c->mask : nullptr;
+        const long long n = c->n;
         for (int it = 0; it < count; ++it) {
+            if constexpr (sizeof(X) == 4) {
+                if (mf) {
+                    enqueue_apply32(c, p, c->mf_ye, &c->cgs->done);
+                    k_mf_gather<X><<<RB, kRedThreads, 0, c->stream>>>(
+                        c->N, c->nadj_ptr, c->nadj, c->mf_ye, p, q, c->mask, c->cgs, c->partials);
+                    k_xr<X><<<RB, kRedThreads, 0, c->stream>>>(n, x, r, p, q, inv, c->cgs,
+                                                               c->partials);
+                    k_p<X><<<RB, kRedThreads, 0, c->stream>>>(n, p, r, inv, c->cgs);
+                    continue;
+                }
+            }
             if (bulk)
                 bulk_kernel<<<bulk_grid, kRedThreads, bulk_smem, c->stream>>>(A, plan, p, q, mask,
                                                                               c->cgs, c->partials);
@@ -721,36 +829,55 @@ static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv,
             k_xr<X><<<RB, kRedThreads, 0, c->stream>>>(n, x, r, p, q, inv, c->cgs, c->partials);
             k_p<X><<<RB, kRedThreads, 0, c->stream>>>(n, p, r, inv, c->cgs);
         }
-    };
-    if (use_graphs && *cache == nullptr) {
-        // capture one block of iterations; fall back to plain launches if the stream cannot be
-        // captured (e.g. the legacy default stream)
-        cudaGraph_t g = nullptr;
-        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-            enqueue(kChunk);
-            if (cudaStreamEndCapture(c->stream, &g) == cudaSuccess && g) {
-                if (cudaGraphInstantiate(cache, g, 0) != cudaSuccess) *cache = nullptr;
-                cudaGraphDestroy(g);
+    }
+
+    // launch blocks of iterations until the scalars say done (bounded by maxit / kChunk + 4)
+    int run(int maxit) {
+        if (use_graphs && *cache == nullptr) {
+            // capture one block of iterations; plain launches if the stream cannot be captured
+            // (e.g. the legacy default stream)
+            cudaGraph_t g = nullptr;
+            if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) ==
+                cudaSuccess) {
+                enqueue(kChunk);
+                if (cudaStreamEndCapture(c->stream, &g) == cudaSuccess && g) {
+                    if (cudaGraphInstantiate(cache, g, 0) != cudaSuccess) *cache = nullptr;
+                    cudaGraphDestroy(g);
+                }
             }
+            cudaGetLastError();
+            if (*cache == nullptr) use_graphs = false;
         }
-        cudaGetLastError();
-        if (*cache == nullptr) use_graphs = false;
-    }
-    int guard = 0;
-    for (;;) {
-        if (use_graphs) {
-            NB2_CUDA(c, cudaGraphLaunch(*cache, c->stream));
-        } else {
-            enqueue(kChunk);
+        int guard = 0;
+        for (;;) {
+            if (use_graphs)
+                NB2_CUDA(c, cudaGraphLaunch(*cache, c->stream));
+            else
+                enqueue(kChunk);
+            c->launches += (mf ? 4 : 3) * kChunk;
+            NB2_TRY(wait_scalars(c));
+            if (c->h_cgs->done) break;
+            if (++guard > (maxit / kChunk) + 4) break;  // scalars say not done: cannot happen
         }
-        c->launches += 3 * kChunk;
-        int st = wait_scalars(c);
-        if (st) return st;
-        if (c->h_cgs->done) break;
-        if (++guard > (maxit / kChunk) + 4) break;  // scalars say not done: cannot happen
+        NB2_CUDA(c, cudaGetLastError());
+        return NB2_OK;
     }
-    NB2_CUDA(c, cudaGetLastError());
-    k_copy_out<X><<<RB, kRedThreads, 0, c->stream>>>(n, x, xout);
+};
+
+template <typename V, typename X>
+static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv, const double* b,
+                      double* xout, double tol, int maxit, bool use_mask, int* iterations,
+                      double* error, bool use_graphs, cudaGraphExec_t* cache) {
+    CgRunner<V, X> cg{c, vals, x, r, p, q, inv, use_mask, use_graphs, cache};
+    NB2_TRY(cg.setup());
+    const long long n = c->n;
+    k_init<X><<<cg.RB, kRedThreads, 0, c->stream>>>(n, b, x, r, p, inv, c->cgs, c->partials, tol);
+    c->launches++;
+    // max_iterations is read by k_xr: set it with a tiny copy
+    NB2_CUDA(c, cudaMemcpyAsync(&c->cgs->max_iterations, &maxit, sizeof(int), cudaMemcpyHostToDevice,
+                                c->stream));
+    NB2_TRY(cg.run(maxit));
+    k_copy_out<X><<<cg.RB, kRedThreads, 0, c->stream>>>(n, x, xout);
     c->launches++;
     const CgScalars& h = *c->h_cgs;
     *iterations = h.iterations;
@@ -758,6 +885,123 @@ static int run_bsr_cg(nb2_ctx* c, const V* vals, X* x, X* r, X* p, X* q, X* inv,
     if (h.status) return h.status;
     if (!h.done) return NB2_E_TIMEOUT;
     return NB2_OK;
+}
+
+// x64[i] += xs[i]; xs[i] = 0 (fold the FP32 increment into the FP64 iterate)
+__global__ void k_fold(long long n, float* __restrict__ xs, double* __restrict__ x64) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        x64[i] += (double)xs[i];
+        xs[i] = 0.0f;
+    }
+}
+
+// r = b - y on free rows, 0 on masked rows; rs = (float) r; reduce r.r (FP64), rs.D^-1 rs
+__global__ void __launch_bounds__(kRedThreads) k_true_residual(
+    long long n, const double* __restrict__ b, const double* __restrict__ y,
+    const unsigned char* __restrict__ mask, const float* __restrict__ inv, float* __restrict__ rs,
+    CgScalars* s, double* partials, double* rr_out) {
+    double acc[2] = {0.0, 0.0};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double ri = mask[i] ? 0.0 : b[i] - y[i];
+        const float rf = (float)ri;
+        rs[i] = rf;
+        acc[0] += ri * ri;
+        acc[1] += (double)rf * (double)(inv[i] * rf);
+    }
+    if (block_partials<2>(acc, partials, &s->counter[3])) {
+        double tot[2];
+        final_sum<2>(partials, tot);
+        if (threadIdx.x == 0) {
+            *rr_out = tot[0];
+            // continue the recurrence with the replaced residual: beta = rz_new / rz_old
+            s->beta = tot[1] / s->abs_new;
+            s->abs_new = tot[1];
+            s->rz = tot[1];
+            s->rr = tot[0];
+            s->counter[3] = 0;
+        }
+    }
+}
+
+// Mixed-precision PCG with reliable updates (residual replacement): the iterations run in FP32
+// on K32 (FP64 dot products); whenever the FP32 residual has dropped by `delta` since the last
+// replacement (or below the final threshold), the FP32 increment is folded into the FP64 iterate
+// x, the true residual b - K x is formed in FP64 with the matrix-free tangent (the operator the
+// FP64 path assembles), and the FP32 residual is replaced by it; the search direction is kept,
+// so the Krylov space is not thrown away as a restarted defect correction does.  Stops when
+// the true residual meets ||r|| < tol ||b|| (the PCG's stop test, linear_solver.cpp:67-109).
+int pcg_reliable_mixed(nb2_ctx* c, const double* b, double* x, double tol, double delta,
+                       int maxit, double* work, int* iterations, bool use_graphs,
+                       bool matrix_free) {
+    CgRunner<float, float> cg{c,         c->K32,      c->cg32_x, c->cg32_r, c->cg32_p,
+                              c->cg32_q, c->cg32_inv, true,      use_graphs,
+                              matrix_free ? &c->graph_mf : &c->graph32};
+    cg.mf = matrix_free;
+    if (matrix_free) {
+        // FP32 operator data and the Jacobi inverse from the stored tangent
+        NB2_TRY(ensure_mf(c));
+        NB2_TRY(launch_mf_setup(c));
+        k_mf_diag<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->nadj_ptr, c->nadj,
+                                                             c->mf_ye, c->cg32_inv);
+        c->launches++;
+    }
+    NB2_TRY(cg.setup());
+    const long long n = c->n;
+    const unsigned grid = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
+    NB2_CUDA(c, cudaMemsetAsync(x, 0, sizeof(double) * n, c->stream));
+    // the first pause comes after a delta reduction of ||b|| (threshold max(tol, delta)^2 b.b)
+    const double t0 = std::max(tol, delta);
+    k_init<float><<<cg.RB, kRedThreads, 0, c->stream>>>(n, b, cg.x, cg.r, cg.p, cg.inv, c->cgs,
+                                                        c->partials, t0);
+    c->launches++;
+    NB2_CUDA(c, cudaMemcpyAsync(&c->cgs->max_iterations, &maxit, sizeof(int),
+                                cudaMemcpyHostToDevice, c->stream));
+    NB2_TRY(wait_scalars(c));
+    const double b2 = c->h_cgs->rhs_norm2;
+    const double thr = std::max(tol * tol * b2, 2.2250738585072014e-308);
+    *iterations = 0;
+    if (b2 == 0.0) return NB2_OK;
+    double* rr_dev = c->norms + 6;
+    for (int update = 0;; ++update) {
+        if (!c->h_cgs->done) NB2_TRY(cg.run(maxit));
+        const CgScalars h = *c->h_cgs;
+        *iterations = h.iterations;
+        if (h.status && h.status != NB2_E_CG_MAXIT) return h.status;
+        // reliable update: x += xs; r = b - K x in FP64
+        k_fold<<<grid, 256, 0, c->stream>>>(n, cg.x, x);
+        NB2_TRY(launch_apply(c, x, work));
+        k_true_residual<<<cg.RB, kRedThreads, 0, c->stream>>>(n, b, work, c->mask, cg.inv, cg.r,
+                                                              c->cgs, c->partials, rr_dev);
+        c->launches += 2;
+        double rr = 0;
+        NB2_CUDA(c, cudaMemcpyAsync(&rr, rr_dev, sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream));
+        NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (std::getenv("NB2_DEBUG"))
+            std::fprintf(stderr, "[nb2] reliable update %d: its %d true |r|^2 %.6e thr %.6e\n",
+                         update, h.iterations, rr, thr);
+        if (!std::isfinite(rr)) return NB2_E_NAN;
+        if (rr < thr) return NB2_OK;
+        if (h.status == NB2_E_CG_MAXIT || h.iterations >= maxit || update > 1000)
+            return NB2_E_CG_MAXIT;
+        // continue: p = D^-1 r + beta p with the replaced residual, next pause after delta
+        const double next = std::max(thr, delta * delta * rr);
+        CgScalars upd = h;
+        upd.threshold = next;
+        upd.done = 0;
+        upd.status = 0;
+        NB2_CUDA(c, cudaMemcpyAsync(&c->cgs->threshold, &upd.threshold, sizeof(double),
+                                    cudaMemcpyHostToDevice, c->stream));
+        NB2_CUDA(c, cudaMemcpyAsync(&c->cgs->done, &upd.done, sizeof(int), cudaMemcpyHostToDevice,
+                                    c->stream));
+        NB2_CUDA(c, cudaMemcpyAsync(&c->cgs->status, &upd.status, sizeof(int),
+                                    cudaMemcpyHostToDevice, c->stream));
+        k_p<float><<<cg.RB, kRedThreads, 0, c->stream>>>(n, cg.p, cg.r, cg.inv, c->cgs);
+        c->launches++;
+        NB2_TRY(wait_scalars(c));
+    }
 }
 
 int pcg_device_fp64(nb2_ctx* c, const double* b, double* x, double tol, int maxit, bool use_mask,
@@ -777,7 +1021,33 @@ int pcg_device_fp32(nb2_ctx* c, const double* b, double* x, double tol, int maxi
 void release_graphs(nb2_ctx* c) {
     if (c->graph64) cudaGraphExecDestroy(c->graph64);
     if (c->graph32) cudaGraphExecDestroy(c->graph32);
-    c->graph64 = c->graph32 = nullptr;
+    if (c->graph_mf) cudaGraphExecDestroy(c->graph_mf);
+    c->graph64 = c->graph32 = c->graph_mf = nullptr;
+}
+
+// y = K v with the FP32 matrix-free operator (v, y device FP64; y unmasked)
+int mf_apply(nb2_ctx* c, const double* v, double* y) {
+    NB2_TRY(ensure_k32(c));
+    NB2_TRY(ensure_mf(c));
+    NB2_TRY(launch_mf_setup(c));
+    const long long n = c->n;
+    k_to_float<<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 8), 256, 0, c->stream>>>(
+        n, v, c->cg32_p);
+    enqueue_apply32(c, c->cg32_p, c->mf_ye, nullptr);
+    k_mf_sum<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->nadj_ptr, c->nadj, c->mf_ye, y);
+    c->launches += 3;
+    NB2_CUDA(c, cudaGetLastError());
+    return NB2_OK;
+}
+
+int ensure_mf(nb2_ctx* c) {
+    if (c->mf_d) return NB2_OK;
+    const long long ev = (long long)c->E * c->npe * 3;
+    NB2_CUDA(c, cudaMalloc(&c->mf_d, sizeof(float) * ev));
+    NB2_CUDA(c, cudaMalloc(&c->mf_ye, sizeof(float) * ev));
+    NB2_CUDA(c, cudaMalloc(&c->mf_c, sizeof(float) * (long long)mf_coefficients(c->mat.model) *
+                                         c->nqp));
+    return build_node_adjacency(c);
 }
 
 void bsr_spmv_fp64(nb2_ctx* c, const double* x, double* y, bool use_mask) {

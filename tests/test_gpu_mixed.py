@@ -44,3 +44,23 @@ def test_mixed_newton_reaches_fp64_solution(api, make):
     u64 = api.StaticMatrix(pr).solve()
     u32 = api.StaticMatrix(pr, precision=api.MIXED, mixed_inner_tolerance=1e-4).solve()
     assert rel_err(u32, u64) < 1e-9
+
+
+@pytest.mark.parametrize("topo", ["hex8", "tet4"])
+@pytest.mark.parametrize("model", list(MATERIALS))
+def test_fp32_matrix_free_tangent(api, topo, model):
+    """The FP32 operator of the mixed PCG equals the assembled FP64 K v to FP32 rounding."""
+    m = M.structured_hex8(4, 3, 3, jitter=0.1, seed=3) if topo == "hex8" else \
+        M.structured_tet4(3, 2, 2)
+    g = api.SolidMesh(m.X, m.conn, MATERIALS[model])
+    g.update_internal_variables(random_displacement(m, SCALE[model], 11))
+    K, _ = g.assemble()
+    rp, col = g.sparsity_pattern()
+    A = sp.csr_matrix((K, col, rp), shape=(g.ndofs, g.ndofs))
+    v = np.random.Generator(np.random.PCG64(9)).standard_normal(g.ndofs)
+    y = g.apply_tangent_fp32(v)
+    assert rel_err(y, A @ v) < 2e-5
+    # the Jacobi diagonal it forms is the assembled diagonal (checked through e_i products)
+    e = np.zeros(g.ndofs)
+    e[7] = 1.0
+    assert abs(g.apply_tangent_fp32(e)[7] - A[7, 7]) <= 1e-5 * abs(A[7, 7])
