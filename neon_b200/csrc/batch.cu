@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -29,6 +30,10 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kBatchChunk = 32;  // CG iterations per captured graph
+// operator / vector precision of the batched PCG
+constexpr int kModeK64 = 0;    // FP64 K, FP64 vectors
+constexpr int kModeK32V32 = 1; // FP32 K, FP32 vectors (FP64 dot products)
+constexpr int kModeK32V64 = 2; // FP32 K, FP64 vectors
 
 struct Tables {
     const int* row0;   // [nchunks] first block row
@@ -344,8 +349,8 @@ __global__ void k_b_element_instance(long long E, int npe, const int* conn, cons
     }
 }
 
-__global__ void k_b_invdiag_f64(const int* brp, const int* bcol, const double* val, int rows,
-                                double* inv) {
+template <typename V, typename X>
+__global__ void k_b_invdiag(const int* brp, const int* bcol, const V* val, int rows, X* inv) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= rows) return;
     int lo = brp[a], hi = brp[a + 1] - 1;
@@ -355,24 +360,8 @@ __global__ void k_b_invdiag_f64(const int* brp, const int* bcol, const double* v
     }
     const bool has = lo < brp[a + 1] && bcol[lo] == a;  // empty row: diagonal 0
     for (int r = 0; r < 3; ++r) {
-        const double d = has ? val[9ll * lo + 4 * r] : 0.0;
-        inv[3ll * a + r] = d != 0.0 ? 1.0 / d : 1.0;
-    }
-}
-
-__global__ void k_b_invdiag_f32(const int* brp, const int* bcol, const float* val, int rows,
-                                float* inv) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= rows) return;
-    int lo = brp[a], hi = brp[a + 1] - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (bcol[mid] < a) lo = mid + 1; else hi = mid;
-    }
-    const bool has = lo < brp[a + 1] && bcol[lo] == a;  // empty row: diagonal 0
-    for (int r = 0; r < 3; ++r) {
-        const float d = has ? val[9ll * lo + 4 * r] : 0.0f;
-        inv[3ll * a + r] = d != 0.0f ? (float)(1.0 / (double)d) : 1.0f;
+        const double d = has ? (double)val[9ll * lo + 4 * r] : 0.0;
+        inv[3ll * a + r] = d != 0.0 ? (X)(1.0 / d) : (X)1;
     }
 }
 
@@ -381,6 +370,40 @@ __global__ void k_b_out(long long n, const X* x, double* out) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
         out[i] = (double)x[i];
+}
+
+// Residual replacement of the flagged instances: r = b - y (FP64, masked rows 0), rs = (X)r;
+// per instance r.r -> rr_out[inst] and the recurrence continued with rz_new = rs.D^-1 rs
+template <typename X>
+__global__ void __launch_bounds__(kThreads) k_b_true_residual(Tables T, const int* flag,
+                                                              const double* __restrict__ b,
+                                                              const double* __restrict__ y,
+                                                              const unsigned char* __restrict__ mask,
+                                                              const X* __restrict__ inv,
+                                                              X* __restrict__ rs, Scalars S,
+                                                              double* part, double* rr_out) {
+    const int inst = T.inst[blockIdx.x];
+    if (!flag[inst]) return;
+    const long long i0 = 3ll * T.row0[blockIdx.x], i1 = 3ll * T.row1[blockIdx.x];
+    double acc[2] = {0.0, 0.0};
+    for (long long i = i0 + threadIdx.x; i < i1; i += kThreads) {
+        const double ri = mask[i] ? 0.0 : b[i] - y[i];
+        const X rf = (X)ri;
+        rs[i] = rf;
+        acc[0] += ri * ri;
+        acc[1] += (double)rf * (double)(inv[i] * rf);
+    }
+    if (chunk_partials<2>(acc, part, &S.ticket[3 * S.ninst + inst], T.count[inst])) {
+        double tot[2];
+        instance_sum<2>(part, T.first[inst], T.count[inst], tot);
+        if (threadIdx.x == 0) {
+            rr_out[inst] = tot[0];
+            S.rr[inst] = tot[0];
+            S.beta[inst] = tot[1] / S.absnew[inst];
+            S.absnew[inst] = tot[1];
+            S.ticket[3 * S.ninst + inst] = 0;
+        }
+    }
 }
 
 unsigned vgrid(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148 * 8); }
@@ -415,7 +438,7 @@ struct BatchState {
     int* flag_b = nullptr;
     std::vector<int> h_done, h_iters, h_status;
     std::vector<double> h_norms;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
 
     Tables tables() const { return Tables{row0, row1, inst, first, count}; }
     Scalars scalars() const {
@@ -535,19 +558,25 @@ int batch_norms(nb2_ctx* c, BatchState* b, const double* v0, const double* v1, c
 
 // Per-instance Jacobi-PCG on the resident K: precision NB2_FP64 (K64, FP64 vectors) or
 // NB2_MIXED (K32, FP32 vectors, FP64 dot products).  Instance i stops at its own tolerance or
-// after maxit[i] iterations; an instance with b = 0 returns x = 0 at once.  x: FP64 solution.
-int batch_pcg(nb2_ctx* c, BatchState* b, int precision, const double* rhs, double* xout,
-              double tol, const std::vector<int>& maxit, bool graphs) {
+// after maxit[i] iterations; an instance with b = 0 returns x = 0 at once.
+//   batch_pcg_start    Jacobi inverse, x = 0, r = b, p = D^-1 r, per-instance thresholds
+//   batch_pcg_iterate  captured blocks of iterations until every instance is done
+int batch_pcg_start(nb2_ctx* c, BatchState* b, int mode, const double* rhs, double tol,
+                    const std::vector<int>& maxit) {
     const Tables T = b->tables();
     const Scalars S = b->scalars();
     const int nb = b->nchunks;
-    const bool f64 = precision == NB2_FP64;
-    if (f64)
-        k_b_invdiag_f64<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->brp, c->bcol, c->K64, c->N,
-                                                                   c->cg_inv);
+    const bool f64 = mode != kModeK32V32;  // FP64 vectors
+    const unsigned g = (c->N + 255) / 256;
+    if (mode == kModeK64)
+        k_b_invdiag<double, double><<<g, 256, 0, c->stream>>>(c->brp, c->bcol, c->K64, c->N,
+                                                              c->cg_inv);
+    else if (mode == kModeK32V64)
+        k_b_invdiag<float, double><<<g, 256, 0, c->stream>>>(c->brp, c->bcol, c->K32, c->N,
+                                                             c->cg_inv);
     else
-        k_b_invdiag_f32<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->brp, c->bcol, c->K32, c->N,
-                                                                   c->cg32_inv);
+        k_b_invdiag<float, float><<<g, 256, 0, c->stream>>>(c->brp, c->bcol, c->K32, c->N,
+                                                            c->cg32_inv);
     NB2_CUDA(c, cudaMemcpyAsync(S.maxit, maxit.data(), sizeof(int) * b->ninst,
                                 cudaMemcpyHostToDevice, c->stream));
     if (f64)
@@ -557,13 +586,27 @@ int batch_pcg(nb2_ctx* c, BatchState* b, int precision, const double* rhs, doubl
         k_b_init<float><<<nb, kThreads, 0, c->stream>>>(T, rhs, c->cg32_x, c->cg32_r, c->cg32_p,
                                                          c->cg32_inv, S, b->part, tol);
     c->launches += 2;
+    NB2_CUDA(c, cudaStreamSynchronize(c->stream));  // maxit's host vector is the caller's
+    return NB2_OK;
+}
+
+int batch_pcg_iterate(nb2_ctx* c, BatchState* b, int mode, int most, bool graphs) {
+    const Tables T = b->tables();
+    const Scalars S = b->scalars();
+    const int nb = b->nchunks;
+    const bool f64 = mode != kModeK32V32;
     const auto spmv64 = spmv_variant<double, double>(b->lanes);
+    const auto spmv3264 = spmv_variant<float, double>(b->lanes);
     const auto spmv32 = spmv_variant<float, float>(b->lanes);
     auto enqueue = [&]() {
         for (int it = 0; it < kBatchChunk; ++it) {
             if (f64) {
-                spmv64<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K64, c->cg_p,
-                                                       c->cg_q, c->mask, S, b->part);
+                if (mode == kModeK64)
+                    spmv64<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K64, c->cg_p,
+                                                           c->cg_q, c->mask, S, b->part);
+                else
+                    spmv3264<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K32, c->cg_p,
+                                                             c->cg_q, c->mask, S, b->part);
                 k_b_xr<double><<<nb, kThreads, 0, c->stream>>>(T, c->cg_x, c->cg_r, c->cg_p,
                                                                c->cg_q, c->cg_inv, S, b->part);
                 k_b_p<double><<<nb, kThreads, 0, c->stream>>>(T, c->cg_p, c->cg_r, c->cg_inv, S);
@@ -577,7 +620,7 @@ int batch_pcg(nb2_ctx* c, BatchState* b, int precision, const double* rhs, doubl
             }
         }
     };
-    cudaGraphExec_t& g = b->graph[f64 ? 0 : 1];
+    cudaGraphExec_t& g = b->graph[mode];
     if (graphs && g == nullptr) {
         cudaGraph_t gr = nullptr;
         if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -590,14 +633,8 @@ int batch_pcg(nb2_ctx* c, BatchState* b, int precision, const double* rhs, doubl
         cudaGetLastError();
     }
     const bool use_graph = graphs && g != nullptr;
-    const int most = *std::max_element(maxit.begin(), maxit.end());
     int guard = 0;
     for (;;) {
-        if (use_graph)
-            NB2_CUDA(c, cudaGraphLaunch(g, c->stream));
-        else
-            enqueue();
-        c->launches += 3 * kBatchChunk;
         NB2_CUDA(c, cudaMemcpyAsync(b->h_done.data(), S.done, sizeof(int) * b->ninst,
                                     cudaMemcpyDeviceToHost, c->stream));
         NB2_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -608,17 +645,32 @@ int batch_pcg(nb2_ctx* c, BatchState* b, int precision, const double* rhs, doubl
             c->error = "batched PCG did not stop within its iteration limit";
             return NB2_E_TIMEOUT;
         }
+        if (use_graph)
+            NB2_CUDA(c, cudaGraphLaunch(g, c->stream));
+        else
+            enqueue();
+        c->launches += 3 * kBatchChunk;
     }
-    if (f64)
-        k_b_out<double><<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->cg_x, xout);
-    else
-        k_b_out<float><<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->cg32_x, xout);
-    c->launches++;
     NB2_CUDA(c, cudaMemcpyAsync(b->h_iters.data(), S.iters, sizeof(int) * b->ninst,
                                 cudaMemcpyDeviceToHost, c->stream));
     NB2_CUDA(c, cudaMemcpyAsync(b->h_status.data(), S.status, sizeof(int) * b->ninst,
                                 cudaMemcpyDeviceToHost, c->stream));
     NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    NB2_CUDA(c, cudaGetLastError());
+    return NB2_OK;
+}
+
+// the whole FP64 solve: start, iterate, x out
+int batch_pcg(nb2_ctx* c, BatchState* b, int mode, const double* rhs, double* xout,
+              double tol, const std::vector<int>& maxit, bool graphs) {
+    NB2_TRY(batch_pcg_start(c, b, mode, rhs, tol, maxit));
+    NB2_TRY(batch_pcg_iterate(c, b, mode, *std::max_element(maxit.begin(), maxit.end()),
+                              graphs));
+    if (mode != kModeK32V32)
+        k_b_out<double><<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->cg_x, xout);
+    else
+        k_b_out<float><<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->cg32_x, xout);
+    c->launches++;
     NB2_CUDA(c, cudaGetLastError());
     return NB2_OK;
 }
@@ -710,7 +762,7 @@ struct BatchNewton {
     int m_dir = 0, m_frc = 0;
     int *e_inst = nullptr, *on = nullptr;
     unsigned* iflags = nullptr;
-    double *rlin = nullptr, *corr = nullptr, *yvec = nullptr;
+    double* yvec = nullptr;  // FP64 product of the residual replacements (mixed)
     std::vector<unsigned> h_iflags;
     double t_elem = 0, t_solve = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -795,68 +847,111 @@ struct BatchNewton {
         reset[i] = 1;  // displacement <- last converged displacement
     }
 
-    // Per-instance defect correction (mixed): FP32 inner PCG on K32, FP64 matrix-free residual
+    // Per-instance mixed precision with reliable updates (the batched counterpart of
+    // pcg_reliable_mixed): iterations on the FP32 K32 with FP64 vectors -- on these nearly
+    // incompressible tet4 systems FP32 vector recurrences cost 50-60% more iterations, while K32
+    // carries most of the bytes -- and when every instance has paused (its recursive residual
+    // fell by delta) or finished, the paused ones get the true residual b - K x with the FP64
+    // tangent (matrix-free, stored coefficients, only their elements) and continue with it,
+    // keeping their search directions.
     int solve_mixed(const std::vector<int>& solving, std::vector<int>& its, std::vector<int>& st) {
         const Tables T = b->tables();
-        const double tol = o.cg_tolerance, inner = o.mixed_inner_tolerance;
-        NB2_TRY(batch_norms(c, b, c->rhs, nullptr, nullptr, nullptr, nullptr));
-        std::vector<double> thr(ninst);
-        std::vector<int> active(ninst, 0);
+        const Scalars S = b->scalars();
+        const double tol = o.cg_tolerance, delta = o.mixed_inner_tolerance;
+        const int maxit = o.cg_maximum_iterations;
+        NB2_CUDA(c, cudaMemsetAsync(b->norms, 0, sizeof(double) * ninst, c->stream));
+        std::vector<int> mx(ninst, maxit);
+        NB2_TRY(batch_pcg_start(c, b, kModeK32V64, c->rhs, std::max(tol, delta), mx));
+        std::vector<double> b2(ninst), thr(ninst), thr_final(ninst), rr(ninst);
+        NB2_CUDA(c, cudaMemcpyAsync(b2.data(), S.rhs2, sizeof(double) * ninst,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        NB2_CUDA(c, cudaMemcpyAsync(thr.data(), S.thr, sizeof(double) * ninst,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+        std::vector<int> finished(ninst), paused(ninst), done(ninst);
         for (int i = 0; i < ninst; ++i) {
-            const double b2 = b->h_norms[i] * b->h_norms[i];
-            thr[i] = std::max(tol * tol * b2, DBL_MIN);
-            active[i] = solving[i] && b2 > 0 && b2 >= thr[i];
+            thr_final[i] = std::max(tol * tol * b2[i], DBL_MIN);
+            finished[i] = !solving[i] || b2[i] == 0.0;
             its[i] = 0;
             st[i] = NB2_OK;
         }
-        NB2_CUDA(c, cudaMemsetAsync(c->du, 0, sizeof(double) * c->n, c->stream));
-        NB2_CUDA(c, cudaMemcpyAsync(rlin, c->rhs, sizeof(double) * c->n, cudaMemcpyDeviceToDevice,
-                                    c->stream));
-        for (int ref = 0; ref < 30 && any(active); ++ref) {
-            NB2_TRY(upload_flags(c, b->flag_a, active));
-            k_b_fill<double><<<b->nchunks, kThreads, 0, c->stream>>>(T, b->flag_a, 0, rlin, 0.0);
-            c->launches++;
-            std::vector<int> mx(ninst, 1);
-            for (int i = 0; i < ninst; ++i)
-                if (active[i]) mx[i] = std::max(1, o.cg_maximum_iterations - its[i]);
-            NB2_TRY(batch_pcg(c, b, NB2_MIXED, rlin, corr, inner, mx, o.use_graphs != 0));
+        for (int update = 0; update < 1000; ++update) {
+            NB2_TRY(batch_pcg_iterate(c, b, kModeK32V64, maxit, o.use_graphs != 0));
             for (int i = 0; i < ninst; ++i) {
-                if (!active[i]) continue;
-                its[i] += b->h_iters[i];
+                paused[i] = 0;
+                if (finished[i]) continue;
+                its[i] = b->h_iters[i];
                 const int s = b->h_status[i];
                 if (s != NB2_OK && s != NB2_E_CG_MAXIT) {
                     st[i] = s;
-                    active[i] = 0;
+                    finished[i] = 1;
+                } else {
+                    paused[i] = 1;
                 }
             }
-            k_b_axpy<<<vgrid(c->n), 256, 0, c->stream>>>(c->n, 1.0, corr, c->du);
-            NB2_TRY(launch_apply(c, c->du, yvec));
-            k_b_sub<<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->rhs, yvec, rlin);
-            k_b_zero_masked<<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->mask, rlin);
-            c->launches += 4;
-            NB2_TRY(batch_norms(c, b, rlin, nullptr, nullptr, nullptr, nullptr));
+            if (!any(paused)) break;
+            NB2_TRY(upload_flags(c, b->flag_a, paused));
+            const int* on_before = c->inst_on;
+            c->inst_on = b->flag_a;  // the FP64 product over the paused instances' elements only
+            const int ap = launch_apply(c, c->cg_x, yvec);
+            c->inst_on = on_before;
+            NB2_TRY(ap);
+            k_b_true_residual<double><<<b->nchunks, kThreads, 0, c->stream>>>(
+                T, b->flag_a, c->rhs, yvec, c->mask, c->cg_inv, c->cg_r, S, b->part, b->norms);
+            c->launches++;
+            NB2_CUDA(c, cudaMemcpyAsync(rr.data(), b->norms, sizeof(double) * ninst,
+                                        cudaMemcpyDeviceToHost, c->stream));
+            NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+            bool restart = false;
             for (int i = 0; i < ninst; ++i) {
-                if (!active[i]) continue;
-                const double r2 = b->h_norms[i] * b->h_norms[i];
-                if (!std::isfinite(r2)) {
+                done[i] = 1;
+                if (!paused[i]) continue;
+                if (!std::isfinite(rr[i])) {
                     st[i] = NB2_E_NAN;
-                    active[i] = 0;
-                } else if (r2 < thr[i]) {
-                    active[i] = 0;
-                } else if (its[i] >= o.cg_maximum_iterations) {
+                    finished[i] = 1;
+                } else if (rr[i] < thr_final[i]) {
+                    finished[i] = 1;
+                } else if (its[i] >= maxit) {
                     st[i] = NB2_E_CG_MAXIT;
-                    active[i] = 0;
+                    finished[i] = 1;
+                } else {
+                    thr[i] = std::max(thr_final[i], delta * delta * rr[i]);
+                    done[i] = 0;
+                    restart = true;
                 }
             }
+            if (std::getenv("NB2_DEBUG")) {
+                int np = 0, nr = 0, mi = 0;
+                double worst = 0.0;
+                for (int i = 0; i < ninst; ++i) {
+                    np += paused[i];
+                    nr += !done[i];
+                    mi = std::max(mi, its[i]);
+                    if (paused[i] && thr_final[i] > 0) worst = std::max(worst, rr[i] / thr_final[i]);
+                }
+                std::fprintf(stderr, "[nb2] batch reliable update %d: paused %d restarted %d max its %d "
+                             "worst rr/thr %.3e\n", update, np, nr, mi, worst);
+            }
+            if (!restart) break;
+            NB2_CUDA(c, cudaMemcpyAsync(S.thr, thr.data(), sizeof(double) * ninst,
+                                        cudaMemcpyHostToDevice, c->stream));
+            NB2_CUDA(c, cudaMemcpyAsync(S.done, done.data(), sizeof(int) * ninst,
+                                        cudaMemcpyHostToDevice, c->stream));
+            k_b_p<double><<<b->nchunks, kThreads, 0, c->stream>>>(T, c->cg_p, c->cg_r, c->cg_inv,
+                                                                  S);
+            c->launches++;
+            NB2_CUDA(c, cudaStreamSynchronize(c->stream));  // host vectors above
         }
         for (int i = 0; i < ninst; ++i)
-            if (active[i]) st[i] = NB2_E_CG_MAXIT;
+            if (!finished[i]) st[i] = NB2_E_CG_MAXIT;
+        k_b_out<double><<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->cg_x, c->du);
+        c->launches++;
         return NB2_OK;
     }
 
     int solve_fp64(const std::vector<int>& solving, std::vector<int>& its, std::vector<int>& st) {
         std::vector<int> mx(ninst, o.cg_maximum_iterations);
-        NB2_TRY(batch_pcg(c, b, NB2_FP64, c->rhs, c->du, o.cg_tolerance, mx, o.use_graphs != 0));
+        NB2_TRY(batch_pcg(c, b, kModeK64, c->rhs, c->du, o.cg_tolerance, mx, o.use_graphs != 0));
         for (int i = 0; i < ninst; ++i) {
             its[i] = solving[i] ? b->h_iters[i] : 0;
             st[i] = solving[i] ? b->h_status[i] : NB2_OK;
@@ -1075,9 +1170,9 @@ extern "C" int nb2_batch_autotune(nb2_ctx* c, int32_t num_instances, const int32
                     spmv_variant<double, double>(L)<<<b->nchunks, kThreads, 0, c->stream>>>(
                         b->tables(), c->brp, c->bcol, c->K64, c->cg_p, c->cg_q, c->mask, S,
                         b->part);
-                else
-                    spmv_variant<float, float>(L)<<<b->nchunks, kThreads, 0, c->stream>>>(
-                        b->tables(), c->brp, c->bcol, c->K32, c->cg32_p, c->cg32_q, c->mask, S,
+                else  // the batched mixed mode: FP32 K, FP64 vectors
+                    spmv_variant<float, double>(L)<<<b->nchunks, kThreads, 0, c->stream>>>(
+                        b->tables(), c->brp, c->bcol, c->K32, c->cg_p, c->cg_q, c->mask, S,
                         b->part);
             };
             sweep();
@@ -1157,8 +1252,6 @@ extern "C" int nb2_batch_static_solve(nb2_ctx* c, int32_t num_instances,
     NB2_TRY(nw.mem.alloc(c, &nw.on, (long long)num_instances));
     NB2_TRY(nw.mem.alloc(c, &nw.iflags, (long long)num_instances));
     if (nw.mixed()) {
-        NB2_TRY(nw.mem.alloc(c, &nw.rlin, (long long)c->n));
-        NB2_TRY(nw.mem.alloc(c, &nw.corr, (long long)c->n));
         NB2_TRY(nw.mem.alloc(c, &nw.yvec, (long long)c->n));
     }
     NB2_CUDA(c, cudaMemsetAsync(d_bad, 0, sizeof(int), c->stream));
