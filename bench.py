@@ -44,6 +44,16 @@ def log(msg):
     print(f"[bench {time.perf_counter() - _T0:8.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
+def max_over_ranks(t, dist, device="cuda"):
+    """The slowest rank's time (every rank gets it); t itself when not distributed."""
+    if dist is None:
+        return t
+    import torch
+    tt = torch.tensor([float(t)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def _env_int(k, d):
     try:
         return int(os.environ.get(k, d))
@@ -279,15 +289,15 @@ def main():
         kernel_ms.append(ev0.elapsed_time(ev1))
     tw1.record(stream)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     launches = mesh.launches() - launches0
     region_ms = tw0.elapsed_time(tw1)
     clock_info = clocks.stop()
     t_asm = sum(kernel_ms) / len(kernel_ms) * 1e-3
     t_max = t_asm
     if dist:
-        tt = torch.tensor([t_asm], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
+        t_max = max_over_ranks(t_asm, dist)
     value = world * E / t_max
 
     # roofline of the dominant kernel (the fused element kernel)
@@ -420,9 +430,7 @@ def end_to_end(api, args, pr, u, world, dist, torch, E):
         e2e_step()
     t_e2e = (time.perf_counter() - t0) / args.e2e_steps
     if dist:
-        tt = torch.tensor([t_e2e], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
+        t_e2e = max_over_ranks(t_e2e, dist)
     e2e = {"value": world * E / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * mesh_e2e.ndofs,
            "d2h_bytes_per_step": 8 * mesh_e2e.nnz + 8 * mesh_e2e.ndofs,
            "call": "nb2_update_internal_variables + nb2_assemble (host u in, host CSR K + f_int "

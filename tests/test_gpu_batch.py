@@ -97,3 +97,19 @@ def test_coupled_instances_are_rejected(api):
     bs.node_offsets = np.array([0, 5, bs.node_offsets[-1]], np.int32)  # cuts instance 0
     with pytest.raises(ValueError):
         bs.solve()
+
+
+def test_batched_hex8_linear_elastic_instances(api):
+    """hex8 instances of different sizes and moduli (config 1 shape) against single solves."""
+    probs = []
+    for n, E in ((3, 200e3), (5, 70e3), (2, 120e3)):
+        pr = P.config_c1(n)
+        nu = 0.3
+        pr.material.K = E / (3 * (1 - 2 * nu))
+        pr.material.G = E / (2 * (1 + nu))
+        probs.append(pr)
+    bs = api.BatchedStaticMatrix(probs, autotune=False)
+    u = bs.solve()
+    for i, pr in enumerate(probs):
+        u1 = api.StaticMatrix(pr).solve()
+        assert rel_err(bs.instance_displacement(i, u), u1) < 1e-10
