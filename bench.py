@@ -415,13 +415,16 @@ def end_to_end(api, args, pr, u, world, dist, torch, E):
     """The metric through the drop-in C-ABI with host buffers, copies inside the timed region."""
     mesh_e2e = api.SolidMesh(pr.mesh.X, pr.mesh.conn, pr.material)
     mesh_e2e.save_internal_variables(True)
-    Kh = np.zeros(mesh_e2e.nnz)
-    fh = np.zeros(mesh_e2e.ndofs)
+    # page-locked host buffers (a caller pins its K value array once, e.g. cudaHostRegister)
+    Kh = torch.zeros(mesh_e2e.nnz, dtype=torch.float64, pin_memory=True).numpy()
+    fh = torch.zeros(mesh_e2e.ndofs, dtype=torch.float64, pin_memory=True).numpy()
+    uh = torch.zeros(mesh_e2e.ndofs, dtype=torch.float64, pin_memory=True).numpy()
+    uh[:] = u
     L = api.lib()
 
     def e2e_step():
         mesh_e2e.save_internal_variables(False)
-        api._check(L.nb2_update_internal_variables(mesh_e2e.h, u.ctypes.data, 0.0), mesh_e2e.h)
+        api._check(L.nb2_update_internal_variables(mesh_e2e.h, uh.ctypes.data, 0.0), mesh_e2e.h)
         api._check(L.nb2_assemble(mesh_e2e.h, Kh.ctypes.data, fh.ctypes.data), mesh_e2e.h)
 
     e2e_step()
@@ -434,7 +437,7 @@ def end_to_end(api, args, pr, u, world, dist, torch, E):
     e2e = {"value": world * E / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * mesh_e2e.ndofs,
            "d2h_bytes_per_step": 8 * mesh_e2e.nnz + 8 * mesh_e2e.ndofs,
            "call": "nb2_update_internal_variables + nb2_assemble (host u in, host CSR K + f_int "
-                   "out)"}
+                   "out; page-locked host buffers)"}
     mesh_e2e.close()
     return e2e
 

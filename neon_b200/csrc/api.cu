@@ -218,7 +218,7 @@ int nb2_destroy(nb2_ctx* c) {
     void* ptrs[] = {c->X,      c->conn,   c->brp,    c->bcol,   c->slot,      c->K64,
                     c->K32,    c->u,      c->u_old,  c->fint,   c->fext,      c->rhs,
                     c->du,     c->inc,    c->mask,   c->Ge,     c->Ke,        c->ep,
-                    c->epbar,  c->u_tan, c->mf_d, c->mf_c, c->mf_ye, c->nadj, c->nadj_ptr,
+                    c->epbar,  c->u_tan, c->Kcsr, c->mf_d, c->mf_c, c->mf_ye, c->nadj, c->nadj_ptr,
                     c->ep_old, c->epbar_old, c->sig, c->dpar,   c->detF,      c->cg_x,
                     c->cg_r,   c->cg_p,   c->cg_q,   c->cg_inv, c->cg32_x,    c->cg32_r,
                     c->cg32_p, c->cg32_q, c->cg32_inv, c->partials, c->cgs,   c->norms,
@@ -339,12 +339,12 @@ int nb2_download_system(nb2_ctx* c, double* K, double* f) {
     if (!c) return NB2_E_INPUT;
     if (K) {
         if (!c->K64) return NB2_E_INPUT;
-        double* tmp = nullptr;
-        NB2_CUDA(c, cudaMallocAsync(&tmp, sizeof(double) * c->nnz, c->stream));
-        NB2_TRY(export_csr_values(c, c->K64, tmp));
-        NB2_CUDA(c, cudaMemcpyAsync(K, tmp, sizeof(double) * c->nnz, cudaMemcpyDeviceToHost,
+        // CSR staging buffer kept for the context's lifetime (one 8 nnz-byte allocation, not one
+        // per call); the copy runs at DMA speed when the caller's buffer is page-locked
+        if (!c->Kcsr) NB2_CUDA(c, cudaMalloc(&c->Kcsr, sizeof(double) * c->nnz));
+        NB2_TRY(export_csr_values(c, c->K64, c->Kcsr));
+        NB2_CUDA(c, cudaMemcpyAsync(K, c->Kcsr, sizeof(double) * c->nnz, cudaMemcpyDeviceToHost,
                                     c->stream));
-        NB2_CUDA(c, cudaFreeAsync(tmp, c->stream));
     }
     if (f)
         NB2_CUDA(c, cudaMemcpyAsync(f, c->fint, sizeof(double) * c->n, cudaMemcpyDeviceToHost,

@@ -98,6 +98,7 @@ struct nb2_ctx {
     // values and vectors
     double* K64 = nullptr;
     float* K32 = nullptr;
+    double* Kcsr = nullptr;  // CSR-ordered copy of K64 for host downloads
     double* u = nullptr;
     double* u_old = nullptr;
     double* fint = nullptr;
