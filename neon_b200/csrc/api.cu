@@ -122,8 +122,7 @@ int nb2::ensure_split_buffers(nb2_ctx* c) {
 
 int nb2::ensure_k32(nb2_ctx* c) {
     if (c->K32) return NB2_OK;
-    // +16 B: the bulk SpMV widens every copy to 16-byte boundaries
-    NB2_TRY(dev_alloc(c, &c->K32, 9 * c->nnzb + 4));
+    NB2_TRY(dev_alloc(c, &c->K32, 9 * c->nnzb));
     NB2_TRY(dev_alloc(c, &c->cg32_x, (long long)c->n));
     NB2_TRY(dev_alloc(c, &c->cg32_r, (long long)c->n));
     NB2_TRY(dev_alloc(c, &c->cg32_p, (long long)c->n));
@@ -134,7 +133,7 @@ int nb2::ensure_k32(nb2_ctx* c) {
 
 int nb2::ensure_k64(nb2_ctx* c) {
     if (c->K64) return NB2_OK;
-    return dev_alloc(c, &c->K64, 9 * c->nnzb + 2);  // +16 B for the bulk SpMV spans
+    return dev_alloc(c, &c->K64, 9 * c->nnzb);
 }
 
 extern "C" {

@@ -157,11 +157,16 @@ __global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restric
 }
 
 // ye[e] = K_e v_e in FP32 from the setup data; skipped once the CG scalars say done.
-// One thread per element: its relative coordinates, input values and output stay in registers
-// and the shape derivatives are constant-memory operands, so the hot loops are FFMA only.  Per
-// point, with D = sum_a d_a (x) dN_a (= J), Gx = sum_a v_a (x) dN_a:
+// One thread per element: its relative coordinates, input values and output stay in registers,
+// so the hot loops are FFMA only.  Per point, with J = sum_a d_a (x) dN_a, Gx = sum_a v_a (x) dN_a:
 //   G = Gx J^-1,  S = s[lam' tr(G) I + mu' (G + G^T) + b (N:G) N + G sigma],  P = S J^-T,
 //   y_a += P dN_a                     (y_a = S L_a with L_a = J^-T dN_a, never formed)
+// hex8 works in the element's trilinear modes (1, xi, eta, zeta, xi eta, xi zeta, eta zeta,
+// xi eta zeta): a +/- butterfly turns the 8 nodal vectors into modal coefficients, the reference
+// gradient at a point is then 4 terms per entry, and the outputs are accumulated per mode and
+// turned back into nodal forces once -- about 30% fewer FMAs than nodal sums at every point.
+// (The factor 1/8 of the trilinear shape functions cancels: J and Gx carry it alike, and
+// P dN_a carries 8 * 1/8.)
 constexpr int kApply32Threads = 128;
 
 template <int NPE>
@@ -172,8 +177,102 @@ __device__ __forceinline__ float dNf(int i) {
         return c_dNf_tet4[i];
 }
 
+// P = S J^-T at one point (J, Gx as defined above, in the same scaling)
+template <int MODEL>
+__device__ __forceinline__ void point_flux(const float* J, const float* Gx,
+                                           const float* __restrict__ mc, long long nqp,
+                                           long long q, float* Pm) {
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
+    constexpr bool kJ2 = (MODEL == MODEL_J2);
+    float Ji[9];
+    inv3f(J, Ji);
+    float G[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            G[i * 3 + k] = Gx[i * 3 + 0] * Ji[0 * 3 + k] + Gx[i * 3 + 1] * Ji[1 * 3 + k] +
+                           Gx[i * 3 + 2] * Ji[2 * 3 + k];
+    const float cl = mc[0 * nqp + q], cm = mc[1 * nqp + q];
+    const float ltr = cl * (G[0] + G[4] + G[8]);
+    float S[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            S[i * 3 + k] = cm * (G[i * 3 + k] + G[k * 3 + i]) + (i == k ? ltr : 0.0f);
+    if constexpr (kJ2) {
+        const float cb = mc[2 * nqp + q];
+        if (cb != 0.0f) {
+            float N6[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) N6[c] = mc[(3 + c) * nqp + q];
+            const float bN = cb * (N6[0] * G[0] + N6[1] * G[4] + N6[2] * G[8] +
+                                   N6[3] * (G[5] + G[7]) + N6[4] * (G[2] + G[6]) +
+                                   N6[5] * (G[1] + G[3]));
+            // N symmetric (11 22 33 23 13 12)
+            S[0] += bN * N6[0]; S[4] += bN * N6[1]; S[8] += bN * N6[2];
+            S[5] += bN * N6[3]; S[7] += bN * N6[3];
+            S[2] += bN * N6[4]; S[6] += bN * N6[4];
+            S[1] += bN * N6[5]; S[3] += bN * N6[5];
+        }
+    }
+    if constexpr (kFinite) {
+        float sg[9];
+        sg[0] = mc[2 * nqp + q]; sg[4] = mc[3 * nqp + q]; sg[8] = mc[4 * nqp + q];
+        sg[5] = sg[7] = mc[5 * nqp + q];
+        sg[2] = sg[6] = mc[6 * nqp + q];
+        sg[1] = sg[3] = mc[7 * nqp + q];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                S[i * 3 + k] += G[i * 3 + 0] * sg[0 * 3 + k] + G[i * 3 + 1] * sg[1 * 3 + k] +
+                                G[i * 3 + 2] * sg[2 * 3 + k];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            Pm[i * 3 + k] = S[i * 3 + 0] * Ji[k * 3 + 0] + S[i * 3 + 1] * Ji[k * 3 + 1] +
+                            S[i * 3 + 2] * Ji[k * 3 + 2];
+}
+
+// modal coefficients (sum_a s_a(m) u_a) of a hex8 nodal 3-vector field, nodes in the reference's
+// corner order; M[0..6] = xi, eta, zeta, xi eta, xi zeta, eta zeta, xi eta zeta (mode 1 unused)
+__device__ __forceinline__ void hex8_modes(const float (&u)[8][3], float (&M)[7][3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float p0 = u[1][c] + u[0][c], m0 = u[1][c] - u[0][c];
+        const float p1 = u[2][c] + u[3][c], m1 = u[2][c] - u[3][c];
+        const float p2 = u[5][c] + u[4][c], m2 = u[5][c] - u[4][c];
+        const float p3 = u[6][c] + u[7][c], m3 = u[6][c] - u[7][c];
+        const float q0 = p1 + p0, q1 = p1 - p0, q2 = p3 + p2, q3 = p3 - p2;
+        const float r0 = m1 + m0, r1 = m1 - m0, r2 = m3 + m2, r3 = m3 - m2;
+        M[0][c] = r2 + r0;  // xi
+        M[1][c] = q3 + q1;  // eta
+        M[2][c] = q2 - q0;  // zeta
+        M[3][c] = r3 + r1;  // xi eta
+        M[4][c] = r2 - r0;  // xi zeta
+        M[5][c] = q3 - q1;  // eta zeta
+        M[6][c] = r3 - r1;  // xi eta zeta
+    }
+}
+
+// reference gradient at (x, e, z): D[i][k] = d u_i / d xi_k (times 8)
+__device__ __forceinline__ void hex8_grad(const float (&M)[7][3], float x, float e, float z,
+                                          float* D) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        D[i * 3 + 0] = M[0][i] + e * M[3][i] + z * M[4][i] + (e * z) * M[6][i];
+        D[i * 3 + 1] = M[1][i] + x * M[3][i] + z * M[5][i] + (x * z) * M[6][i];
+        D[i * 3 + 2] = M[2][i] + x * M[4][i] + e * M[5][i] + (x * e) * M[6][i];
+    }
+}
+
 template <int NPE, int MODEL>
-__global__ void __launch_bounds__(kApply32Threads) k_apply32(int E, const int* __restrict__ conn,
+__global__ void __launch_bounds__(kApply32Threads, (MODEL == MODEL_J2 || MODEL == MODEL_LE) ? 4 : 1)
+k_apply32(int E, const int* __restrict__ conn,
                                                              const float* __restrict__ md,
                                                              const float* __restrict__ mc,
                                                              long long nqp,
@@ -182,8 +281,6 @@ __global__ void __launch_bounds__(kApply32Threads) k_apply32(int E, const int* _
                                                              const int* __restrict__ done) {
     using T = Topo<NPE>;
     constexpr int NQ = T::NQ;
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
-    constexpr bool kJ2 = (MODEL == MODEL_J2);
     if (done && *done) return;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= E) return;
@@ -209,85 +306,85 @@ __global__ void __launch_bounds__(kApply32Threads) k_apply32(int E, const int* _
                 for (int k = 0; k < 3; ++k) vv[4 * j + b][k] = v[3ll * nd[b] + k];
         }
     }
+    if constexpr (NPE == 8) {
+        float Md[7][3], Mv[7][3], Y[7][3];
+        hex8_modes(d, Md);
+        hex8_modes(vv, Mv);
 #pragma unroll
-    for (int a = 0; a < NPE; ++a) y[a][0] = y[a][1] = y[a][2] = 0.0f;
+        for (int m = 0; m < 7; ++m) Y[m][0] = Y[m][1] = Y[m][2] = 0.0f;
+        constexpr float g = 0.57735026918962576f;  // 1/sqrt(3): the 2-point Gauss abscissa
 #pragma unroll
-    for (int l = 0; l < NQ; ++l) {
-        const long long q = e * NQ + l;
-        float J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        float Gx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int l = 0; l < 8; ++l) {
+            // point l has the signs of corner l (hexahedron_quadrature.cpp order)
+            const float x = ((l == 1) || (l == 2) || (l == 5) || (l == 6)) ? g : -g;
+            const float ee = ((l == 2) || (l == 3) || (l == 6) || (l == 7)) ? g : -g;
+            const float z = (l >= 4) ? g : -g;
+            float J[9], Gx[9], Pm[9];
+            hex8_grad(Md, x, ee, z, J);
+            hex8_grad(Mv, x, ee, z, Gx);
+            point_flux<MODEL>(J, Gx, mc, nqp, e * 8 + l, Pm);
+            const float ez = ee * z, xz = x * z, xe = x * ee;
 #pragma unroll
-        for (int a = 0; a < NPE; ++a)
+            for (int i = 0; i < 3; ++i) {
+                const float P0 = Pm[i * 3 + 0], P1 = Pm[i * 3 + 1], P2 = Pm[i * 3 + 2];
+                Y[0][i] += P0;
+                Y[1][i] += P1;
+                Y[2][i] += P2;
+                Y[3][i] += ee * P0 + x * P1;
+                Y[4][i] += z * P0 + x * P2;
+                Y[5][i] += z * P1 + ee * P2;
+                Y[6][i] += ez * P0 + xz * P1 + xe * P2;
+            }
+        }
+        // back to nodes: y_a = sum_m s_a(m) Y_m (transposed butterfly; mode 1 carries nothing)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float g = dNf<NPE>((l * NPE + a) * 3 + k);
+        for (int c = 0; c < 3; ++c) {
+            const float a0_1 = -Y[2][c], a1_1 = Y[2][c];           // 1 -/+ zeta
+            const float a0_e = Y[1][c] - Y[5][c], a1_e = Y[1][c] + Y[5][c];
+            const float a0_x = Y[0][c] - Y[4][c], a1_x = Y[0][c] + Y[4][c];
+            const float a0_xe = Y[3][c] - Y[6][c], a1_xe = Y[3][c] + Y[6][c];
+            // z = 0 corners 0..3, z = 1 corners 4..7
+            const float b00_1 = a0_1 - a0_e, b01_1 = a0_1 + a0_e;   // (y=0 / y=1, z=0)
+            const float b00_x = a0_x - a0_xe, b01_x = a0_x + a0_xe;
+            const float b10_1 = a1_1 - a1_e, b11_1 = a1_1 + a1_e;   // (y=0 / y=1, z=1)
+            const float b10_x = a1_x - a1_xe, b11_x = a1_x + a1_xe;
+            y[0][c] = b00_1 - b00_x;  // (x0 y0 z0)
+            y[1][c] = b00_1 + b00_x;  // (x1 y0 z0)
+            y[2][c] = b01_1 + b01_x;  // (x1 y1 z0)
+            y[3][c] = b01_1 - b01_x;  // (x0 y1 z0)
+            y[4][c] = b10_1 - b10_x;  // (x0 y0 z1)
+            y[5][c] = b10_1 + b10_x;  // (x1 y0 z1)
+            y[6][c] = b11_1 + b11_x;  // (x1 y1 z1)
+            y[7][c] = b11_1 - b11_x;  // (x0 y1 z1)
+        }
+    } else {
 #pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    J[i * 3 + k] += d[a][i] * g;
-                    Gx[i * 3 + k] += vv[a][i] * g;
+        for (int a = 0; a < NPE; ++a) y[a][0] = y[a][1] = y[a][2] = 0.0f;
+#pragma unroll
+        for (int l = 0; l < NQ; ++l) {
+            float J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            float Gx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int a = 0; a < NPE; ++a)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float gk = dNf<NPE>((l * NPE + a) * 3 + k);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        J[i * 3 + k] += d[a][i] * gk;
+                        Gx[i * 3 + k] += vv[a][i] * gk;
+                    }
                 }
+            float Pm[9];
+            point_flux<MODEL>(J, Gx, mc, nqp, e * NQ + l, Pm);
+#pragma unroll
+            for (int a = 0; a < NPE; ++a) {
+                const float g0 = dNf<NPE>((l * NPE + a) * 3 + 0), g1 = dNf<NPE>((l * NPE + a) * 3 + 1),
+                            g2 = dNf<NPE>((l * NPE + a) * 3 + 2);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    y[a][i] += Pm[i * 3 + 0] * g0 + Pm[i * 3 + 1] * g1 + Pm[i * 3 + 2] * g2;
             }
-        float Ji[9];
-        inv3f(J, Ji);
-        float G[9];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-                G[i * 3 + k] = Gx[i * 3 + 0] * Ji[0 * 3 + k] + Gx[i * 3 + 1] * Ji[1 * 3 + k] +
-                               Gx[i * 3 + 2] * Ji[2 * 3 + k];
-        const float cl = mc[0 * nqp + q], cm = mc[1 * nqp + q];
-        const float ltr = cl * (G[0] + G[4] + G[8]);
-        float S[9];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-                S[i * 3 + k] = cm * (G[i * 3 + k] + G[k * 3 + i]) + (i == k ? ltr : 0.0f);
-        if constexpr (kJ2) {
-            const float cb = mc[2 * nqp + q];
-            if (cb != 0.0f) {
-                float N6[6];
-#pragma unroll
-                for (int c = 0; c < 6; ++c) N6[c] = mc[(3 + c) * nqp + q];
-                const float bN = cb * (N6[0] * G[0] + N6[1] * G[4] + N6[2] * G[8] +
-                                       N6[3] * (G[5] + G[7]) + N6[4] * (G[2] + G[6]) +
-                                       N6[5] * (G[1] + G[3]));
-                // N symmetric (11 22 33 23 13 12)
-                S[0] += bN * N6[0]; S[4] += bN * N6[1]; S[8] += bN * N6[2];
-                S[5] += bN * N6[3]; S[7] += bN * N6[3];
-                S[2] += bN * N6[4]; S[6] += bN * N6[4];
-                S[1] += bN * N6[5]; S[3] += bN * N6[5];
-            }
-        }
-        if constexpr (kFinite) {
-            float sg[9];
-            sg[0] = mc[2 * nqp + q]; sg[4] = mc[3 * nqp + q]; sg[8] = mc[4 * nqp + q];
-            sg[5] = sg[7] = mc[5 * nqp + q];
-            sg[2] = sg[6] = mc[6 * nqp + q];
-            sg[1] = sg[3] = mc[7 * nqp + q];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    S[i * 3 + k] += G[i * 3 + 0] * sg[0 * 3 + k] + G[i * 3 + 1] * sg[1 * 3 + k] +
-                                    G[i * 3 + 2] * sg[2 * 3 + k];
-        }
-        // P = S J^-T: P[i][k] = sum_j S[i][j] Ji[k][j]
-        float Pm[9];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-                Pm[i * 3 + k] = S[i * 3 + 0] * Ji[k * 3 + 0] + S[i * 3 + 1] * Ji[k * 3 + 1] +
-                                S[i * 3 + 2] * Ji[k * 3 + 2];
-#pragma unroll
-        for (int a = 0; a < NPE; ++a) {
-            const float g0 = dNf<NPE>((l * NPE + a) * 3 + 0), g1 = dNf<NPE>((l * NPE + a) * 3 + 1),
-                        g2 = dNf<NPE>((l * NPE + a) * 3 + 2);
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-                y[a][i] += Pm[i * 3 + 0] * g0 + Pm[i * 3 + 1] * g1 + Pm[i * 3 + 2] * g2;
         }
     }
     float4* o4 = reinterpret_cast<float4*>(ye + e * NPE * 3);

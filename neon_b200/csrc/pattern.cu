@@ -93,7 +93,7 @@ int build_pattern(nb2_ctx* c) {
     int* count = nullptr;
     NB2_CUDA(c, cudaMallocAsync(&count, sizeof(int) * (c->N + 1), c->stream));
     NB2_CUDA(c, cudaMemsetAsync(count, 0, sizeof(int) * (c->N + 1), c->stream));
-    NB2_CUDA(c, cudaMalloc(&c->bcol, sizeof(int) * (m + 4)));  // +16 B for the bulk SpMV
+    NB2_CUDA(c, cudaMalloc(&c->bcol, sizeof(int) * m));
     NB2_CUDA(c, cudaMalloc(&c->brp, sizeof(int) * (c->N + 1)));
     k_split_keys<<<(unsigned)((m + T - 1) / T), T, 0, c->stream>>>(keys, m, count, c->bcol);
     c->launches++;

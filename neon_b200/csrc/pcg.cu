@@ -9,9 +9,9 @@
 //
 // Here K stays resident in HBM and every scalar stays on the device.  One iteration is three
 // kernels:
-//   k_spmv  : q = A p over the 3x3 block rows (one warp per block row, values streamed with
-//             evict-first loads so p stays in L2), fused with the p.q reduction; the last block
-//             to finish forms alpha = (r.z)/(p.q);
+//   k_spmv  : q = A p over the 3x3 block rows (a few lanes per block row, several rows per
+//             warp in flight), fused with the p.q reduction; the last block to finish forms
+//             alpha = (r.z)/(p.q);
 //   k_xr    : x += alpha p, r -= alpha q, fused with r.r and r.z (z = D^-1 r); the last block
 //             applies the stop test, beta and the iteration count;
 //   k_p     : p = D^-1 r + beta p.
@@ -21,6 +21,7 @@
 // Rows of active Dirichlet DOFs are skipped (q = 0): with b = 0 there, r, z, p stay exactly 0 on
 // them, so this equals neon's zeroing of those rows and columns (static_matrix.hpp:279-320).
 #include <cfloat>
+#include <cstdint>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -167,21 +168,46 @@ __device__ __forceinline__ void bsr_row(const Bsr<V>& A, const X* __restrict__ x
 // ---------------------------------------------------------------------------------------
 // CG kernels (BSR)
 // ---------------------------------------------------------------------------------------
-template <typename V, typename X>
+// q = A p with LPR lanes per 3x3 block row: a warp keeps 32/LPR rows in flight; lane l of a row
+// walks its blocks l, l+LPR, ... (9 values, the block column, 3 gathered p entries) and the three
+// row sums are reduced over the LPR lanes with shuffles.  Plain loads with many independent rows
+// per SM stream the matrix at ~80% of HBM bandwidth (hex8 rows: 27 blocks, tet4: ~15), where a
+// whole warp per row or a shared-memory staging pipeline left it latency-bound.  Fused with the
+// p.q reduction; the last block forms alpha = (r.z)/(p.q).
+template <typename V, typename X, int LPR>
 __global__ void __launch_bounds__(kRedThreads) k_spmv(Bsr<V> A, const X* __restrict__ p,
                                                       X* __restrict__ q,
                                                       const unsigned char* __restrict__ mask,
                                                       CgScalars* s, double* partials) {
     if (s->done) return;
-    const int lane = threadIdx.x & 31;
-    const int warps = gridDim.x * (blockDim.x >> 5);
+    constexpr int RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31, sub = lane / LPR, sl = lane % LPR;
+    const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
     double dot[1] = {0.0};
-    for (int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); a < A.rows; a += warps) {
-        X y0, y1, y2;
-        bsr_row<V, X, X>(A, p, a, lane, y0, y1, y2);
-        if (lane < 3) {
-            const long long i = 3ll * a + lane;
-            X y = lane == 0 ? y0 : (lane == 1 ? y1 : y2);
+    for (long long a0 = gw * RPW; a0 < A.rows; a0 += nw * RPW) {
+        const long long a = a0 + sub;
+        X y0 = 0, y1 = 0, y2 = 0;
+        if (a < A.rows) {
+            const int b0 = A.brp[a], b1 = A.brp[a + 1];
+            for (int k = b0 + sl; k < b1; k += LPR) {
+                const long long col = A.bcol[k];
+                const X x0 = p[3 * col], x1 = p[3 * col + 1], x2 = p[3 * col + 2];
+                const V* blk = A.val + 9ll * k;
+                y0 += (X)blk[0] * x0 + (X)blk[1] * x1 + (X)blk[2] * x2;
+                y1 += (X)blk[3] * x0 + (X)blk[4] * x1 + (X)blk[5] * x2;
+                y2 += (X)blk[6] * x0 + (X)blk[7] * x1 + (X)blk[8] * x2;
+            }
+        }
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) {
+            y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+            y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+        }
+        if (a < A.rows && sl < 3) {
+            const long long i = 3 * a + sl;
+            X y = sl == 0 ? y0 : (sl == 1 ? y1 : y2);
             if (mask && mask[i]) y = (X)0;
             q[i] = y;
             dot[0] += (double)p[i] * (double)y;
@@ -204,221 +230,42 @@ __global__ void __launch_bounds__(kRedThreads) k_spmv(Bsr<V> A, const X* __restr
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// Bulk-copy pipelined SpMV (sm_100a).  A block row's values ([deg][9]) and block columns are
-// contiguous, and so is a chunk of R consecutive block rows.  One elected thread streams the
-// chunks a CTA owns into a ring of shared-memory stages with cp.async.bulk (completion on an
-// mbarrier, L2 evict-first so the gathered vector stays resident), while the 8 warps compute on
-// the stage that has landed: lane = block of the row, 9 values from shared memory, the 3 x
-// entries of the block column from L2, 3 partial row sums reduced across the warp.  Every wait
-// on an mbarrier is bounded: on expiry the kernel records NB2_E_TIMEOUT and stops issuing.
-// ---------------------------------------------------------------------------------------
-constexpr int kStages = 3;
-constexpr unsigned kWaitLimit = 1u << 22;
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-    for (unsigned i = 0; i < kWaitLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
-                                          unsigned long long* bar, unsigned long long policy) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
-        "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
-        : "memory");
+// lanes per block row of the PCG SpMV (measured on B200: FP64 values 4, FP32 values 8)
+template <typename V>
+constexpr int spmv_lanes() {
+    return sizeof(V) == 8 ? 4 : 8;
 }
 
-struct BulkPlan {
-    int rows_per_chunk;
-    int chunks;
-    int stage_val_bytes;  // per stage, 16-byte multiple
-    int stage_col_bytes;
+// 16-byte vector view of the CG vectors (float4 / double2): the update kernels move W values
+// per load and store when every vector is 16-byte aligned (device allocations are; a caller's
+// buffers may not be, then the scalar loop does all of it)
+template <typename X>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    using T = float4;
+    static constexpr int W = 4;
+};
+template <>
+struct Vec16<double> {
+    using T = double2;
+    static constexpr int W = 2;
 };
 
-// byte range [lo, hi) of elements [b0, b1) of an array of `size`-byte items, widened to 16 B
-__device__ __forceinline__ void span16(long long b0, long long b1, int size, long long& lo,
-                                       long long& hi) {
-    lo = (b0 * size) & ~15ll;
-    hi = (b1 * size + 15) & ~15ll;
+__device__ __forceinline__ bool aligned16(const void* a, const void* b, const void* c,
+                                          const void* d, const void* e) {
+    return ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) |
+             reinterpret_cast<uintptr_t>(c) | reinterpret_cast<uintptr_t>(d) |
+             reinterpret_cast<uintptr_t>(e)) & 15) == 0;
 }
 
-template <typename V, typename X, int RPW>
-__global__ void __launch_bounds__(kRedThreads) k_spmv_bulk(Bsr<V> A, BulkPlan plan,
-                                                           const X* __restrict__ p,
-                                                           X* __restrict__ q,
-                                                           const unsigned char* __restrict__ mask,
-                                                           CgScalars* s, double* partials) {
-    if (s->done) return;
-    extern __shared__ __align__(128) unsigned char dyn[];
-    __shared__ unsigned long long bar[kStages];
-    __shared__ int timed_out;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    unsigned char* stage_base[kStages];
-#pragma unroll
-    for (int i = 0; i < kStages; ++i)
-        stage_base[i] = dyn + i * (plan.stage_val_bytes + plan.stage_col_bytes);
-    unsigned long long policy = 0;
-    if (tid == 0) {
-        for (int i = 0; i < kStages; ++i) mbar_init(&bar[i], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
-        timed_out = 0;
-    }
-    __syncthreads();
-    // chunks of this CTA: blockIdx.x, blockIdx.x + gridDim.x, ...
-    const int my_chunks = (plan.chunks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
-    auto issue = [&](int j) {  // thread 0 only
-        const int c = blockIdx.x + j * gridDim.x;
-        const int r0 = c * plan.rows_per_chunk;
-        const int r1 = min(r0 + plan.rows_per_chunk, A.rows);
-        const long long b0 = A.brp[r0], b1 = A.brp[r1];
-        long long vlo, vhi, clo, chi;
-        span16(9 * b0, 9 * b1, (int)sizeof(V), vlo, vhi);
-        span16(b0, b1, 4, clo, chi);
-        const int st = j % kStages;
-        unsigned char* dst = stage_base[st];
-        mbar_expect_tx(&bar[st], (unsigned)((vhi - vlo) + (chi - clo)));
-        bulk_load(dst, reinterpret_cast<const unsigned char*>(A.val) + vlo, (unsigned)(vhi - vlo),
-                  &bar[st], policy);
-        bulk_load(dst + plan.stage_val_bytes, reinterpret_cast<const unsigned char*>(A.bcol) + clo,
-                  (unsigned)(chi - clo), &bar[st], policy);
-    };
-    int last_issued = -1;  // thread 0 only
-    if (tid == 0)
-        for (int j = 0; j < kStages - 1 && j < my_chunks; ++j) {
-            issue(j);
-            last_issued = j;
-        }
-    double dot[1] = {0.0};
-    int consumed = -1;
-    for (int j = 0; j < my_chunks; ++j) {
-        const int st = j % kStages;
-        const bool stop = timed_out != 0;  // stable: written only before a __syncthreads
-        if (tid == 0 && j + kStages - 1 < my_chunks && !stop) {
-            // the stage being refilled was read in iteration j-1 (all threads passed the
-            // barrier below); order those generic reads before the async-proxy writes
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(j + kStages - 1);
-            last_issued = j + kStages - 1;
-        }
-        const unsigned parity = (unsigned)((j / kStages) & 1);
-        if (!stop && !mbar_wait(&bar[st], parity)) atomicExch(&timed_out, 1);
-        __syncthreads();
-        if (!timed_out) {
-            consumed = j;
-            const int c = blockIdx.x + j * gridDim.x;
-            const int r0 = c * plan.rows_per_chunk;
-            const int r1 = min(r0 + plan.rows_per_chunk, A.rows);
-            const long long cb0 = A.brp[r0];
-            const long long voff = (9 * cb0 * (long long)sizeof(V)) & 15ll;  // bytes
-            const long long coff = (cb0 * 4) & 15ll;
-            const V* sv = reinterpret_cast<const V*>(stage_base[st] + voff);
-            const int* sc = reinterpret_cast<const int*>(stage_base[st] + plan.stage_val_bytes + coff);
-            // each warp owns RPW consecutive rows of the chunk and keeps all of them in flight:
-            // block columns and x gathers of every row are issued before any arithmetic
-            const int rbase = r0 + warp * RPW;
-            int rbv[RPW], degv[RPW], colv[RPW];
-            X xv[RPW][3], pv[RPW];
-#pragma unroll
-            for (int t = 0; t < RPW; ++t) {
-                const int row = rbase + t;
-                const bool ok = row < r1;
-                rbv[t] = ok ? A.brp[row] - (int)cb0 : 0;
-                degv[t] = ok ? A.brp[row + 1] - A.brp[row] : 0;
-                colv[t] = lane < degv[t] ? sc[rbv[t] + lane] : 0;
-            }
-#pragma unroll
-            for (int t = 0; t < RPW; ++t) {
-                const bool act = lane < degv[t];
-                xv[t][0] = act ? __ldg(p + 3ll * colv[t]) : (X)0;
-                xv[t][1] = act ? __ldg(p + 3ll * colv[t] + 1) : (X)0;
-                xv[t][2] = act ? __ldg(p + 3ll * colv[t] + 2) : (X)0;
-                pv[t] = (lane < 3 && degv[t] > 0) ? p[3ll * (rbase + t) + lane] : (X)0;
-            }
-            X acc[RPW][3];
-#pragma unroll
-            for (int t = 0; t < RPW; ++t) {
-                acc[t][0] = acc[t][1] = acc[t][2] = (X)0;
-                if (lane < degv[t]) {
-                    const V* blk = sv + 9 * (rbv[t] + lane);
-                    acc[t][0] = (X)blk[0] * xv[t][0] + (X)blk[1] * xv[t][1] + (X)blk[2] * xv[t][2];
-                    acc[t][1] = (X)blk[3] * xv[t][0] + (X)blk[4] * xv[t][1] + (X)blk[5] * xv[t][2];
-                    acc[t][2] = (X)blk[6] * xv[t][0] + (X)blk[7] * xv[t][1] + (X)blk[8] * xv[t][2];
-                }
-                for (int k = lane + 32; k < degv[t]; k += 32) {  // rows of more than 32 blocks
-                    const int col = sc[rbv[t] + k];
-                    const X x0 = __ldg(p + 3ll * col), x1 = __ldg(p + 3ll * col + 1),
-                            x2 = __ldg(p + 3ll * col + 2);
-                    const V* blk = sv + 9 * (rbv[t] + k);
-                    acc[t][0] += (X)blk[0] * x0 + (X)blk[1] * x1 + (X)blk[2] * x2;
-                    acc[t][1] += (X)blk[3] * x0 + (X)blk[4] * x1 + (X)blk[5] * x2;
-                    acc[t][2] += (X)blk[6] * x0 + (X)blk[7] * x1 + (X)blk[8] * x2;
-                }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                for (int t = 0; t < RPW; ++t)
-#pragma unroll
-                    for (int r = 0; r < 3; ++r)
-                        acc[t][r] += __shfl_xor_sync(0xffffffffu, acc[t][r], o);
-#pragma unroll
-            for (int t = 0; t < RPW; ++t) {
-                if (lane < 3 && degv[t] > 0) {
-                    const long long i = 3ll * (rbase + t) + lane;
-                    X y = lane == 0 ? acc[t][0] : (lane == 1 ? acc[t][1] : acc[t][2]);
-                    if (mask && mask[i]) y = (X)0;
-                    q[i] = y;
-                    dot[0] += (double)pv[t] * (double)y;
-                }
-            }
-        }
-        __syncthreads();  // stage st is free for the producer
-    }
-    if (timed_out && tid == 0) {
-        // let the copies still in flight land before the CTA exits (bounded waits)
-        for (int j = consumed + 1; j <= last_issued; ++j)
-            mbar_wait(&bar[j % kStages], (unsigned)((j / kStages) & 1));
-        s->status = NB2_E_TIMEOUT;
-        s->done = 1;
-    }
-    if (block_partials<1>(dot, partials, &s->counter[0])) {
-        double tot[1];
-        final_sum<1>(partials, tot);
-        if (threadIdx.x == 0) {
-            s->pq = tot[0];
-            s->alpha = s->abs_new / tot[0];
-            if (!isfinite(s->alpha)) {
-                s->status = NB2_E_NAN;
-                s->done = 1;
-            }
-            s->counter[0] = 0;
-        }
-    }
+template <typename X>
+__device__ __forceinline__ void xr_one(X& x, X& r, X p, X q, X inv, X alpha, double (&acc)[2]) {
+    x += alpha * p;
+    const X ri = r - alpha * q;
+    r = ri;
+    acc[0] += (double)ri * (double)ri;
+    acc[1] += (double)ri * (double)(inv * ri);
 }
 
 template <typename X>
@@ -428,16 +275,26 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(long long n, X* __restrict__
                                                     const X* __restrict__ inv, CgScalars* s,
                                                     double* partials) {
     if (s->done) return;
+    using V = typename Vec16<X>::T;
+    constexpr int W = Vec16<X>::W;
     const X alpha = (X)s->alpha;
     double acc[2] = {0.0, 0.0};
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        x[i] += alpha * p[i];
-        X ri = r[i] - alpha * q[i];
-        r[i] = ri;
-        acc[0] += (double)ri * (double)ri;
-        acc[1] += (double)ri * (double)(inv[i] * ri);
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long st = (long long)gridDim.x * blockDim.x;
+    const long long nv = aligned16(x, r, p, q, inv) ? n / W : 0;
+    for (long long j = t0; j < nv; j += st) {
+        X xv[W], rv[W], pv[W], qv[W], iv[W];
+        *reinterpret_cast<V*>(xv) = reinterpret_cast<const V*>(x)[j];
+        *reinterpret_cast<V*>(rv) = reinterpret_cast<const V*>(r)[j];
+        *reinterpret_cast<V*>(pv) = reinterpret_cast<const V*>(p)[j];
+        *reinterpret_cast<V*>(qv) = reinterpret_cast<const V*>(q)[j];
+        *reinterpret_cast<V*>(iv) = reinterpret_cast<const V*>(inv)[j];
+#pragma unroll
+        for (int w = 0; w < W; ++w) xr_one(xv[w], rv[w], pv[w], qv[w], iv[w], alpha, acc);
+        reinterpret_cast<V*>(x)[j] = *reinterpret_cast<V*>(xv);
+        reinterpret_cast<V*>(r)[j] = *reinterpret_cast<V*>(rv);
     }
+    for (long long i = nv * W + t0; i < n; i += st) xr_one(x[i], r[i], p[i], q[i], inv[i], alpha, acc);
     if (block_partials<2>(acc, partials, &s->counter[1])) {
         double tot[2];
         final_sum<2>(partials, tot);
@@ -469,10 +326,22 @@ __global__ void __launch_bounds__(kRedThreads) k_p(long long n, X* __restrict__ 
                                                    const X* __restrict__ r,
                                                    const X* __restrict__ inv, const CgScalars* s) {
     if (s->done) return;
+    using V = typename Vec16<X>::T;
+    constexpr int W = Vec16<X>::W;
     const X beta = (X)s->beta;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x)
-        p[i] = inv[i] * r[i] + beta * p[i];
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long st = (long long)gridDim.x * blockDim.x;
+    const long long nv = aligned16(p, r, inv, p, r) ? n / W : 0;
+    for (long long j = t0; j < nv; j += st) {
+        X pv[W], rv[W], iv[W];
+        *reinterpret_cast<V*>(pv) = reinterpret_cast<const V*>(p)[j];
+        *reinterpret_cast<V*>(rv) = reinterpret_cast<const V*>(r)[j];
+        *reinterpret_cast<V*>(iv) = reinterpret_cast<const V*>(inv)[j];
+#pragma unroll
+        for (int w = 0; w < W; ++w) pv[w] = iv[w] * rv[w] + beta * pv[w];
+        reinterpret_cast<V*>(p)[j] = *reinterpret_cast<V*>(pv);
+    }
+    for (long long i = nv * W + t0; i < n; i += st) p[i] = inv[i] * r[i] + beta * p[i];
 }
 
 // x = 0, r = b (as X), p = D^-1 r; rhs_norm2, r.r, r.p; threshold and early exits.
@@ -735,34 +604,9 @@ static int wait_scalars(nb2_ctx* c) {
 }
 
 constexpr int kChunk = 32;
-constexpr int kBulkSmemBudget = 200 * 1024;  // per CTA
-constexpr int kBulkWarps = kRedThreads / 32;
 
-// Rows per chunk and stage sizes of the bulk SpMV: 8 warps x RPW rows with the largest RPW in
-// {8, 4, 2, 1} whose kStages stages fit the shared-memory budget (spans widened to 16 B as the
-// copies are).
-static bool make_bulk_plan(const nb2_ctx* c, int vsize, BulkPlan* plan) {
-    for (int R = 8 * kBulkWarps; R >= kBulkWarps; R /= 2) {
-        long long maxv = 0, maxc = 0;
-        const int chunks = (c->N + R - 1) / R;
-        for (int ch = 0; ch < chunks; ++ch) {
-            const long long b0 = c->h_brp[(size_t)ch * R];
-            const long long b1 = c->h_brp[std::min((size_t)(ch + 1) * R, (size_t)c->N)];
-            const long long vlo = (9 * b0 * vsize) & ~15ll, vhi = (9 * b1 * vsize + 15) & ~15ll;
-            const long long clo = (b0 * 4) & ~15ll, chi = (b1 * 4 + 15) & ~15ll;
-            maxv = std::max(maxv, vhi - vlo);
-            maxc = std::max(maxc, chi - clo);
-        }
-        if (kStages * (maxv + maxc) <= kBulkSmemBudget) {
-            *plan = BulkPlan{R, chunks, (int)maxv, (int)maxc};
-            return true;
-        }
-    }
-    return false;
-}
-
-// One Jacobi-PCG on a block matrix: the bulk SpMV plan, the captured block of kChunk iterations
-// and the host loop that launches blocks until the device scalars say done.
+// One Jacobi-PCG on a block matrix: the captured block of kChunk iterations and the host loop
+// that launches blocks until the device scalars say done.
 template <typename V, typename X>
 struct CgRunner {
     nb2_ctx* c;
@@ -773,33 +617,11 @@ struct CgRunner {
     bool mf = false;  // FP32 matrix-free operator (V = X = float) instead of the assembled K
     int RB = 0;
     Bsr<V> A{};
-    BulkPlan plan{};
-    bool bulk = false;
-    int bulk_grid = 0;
-    size_t bulk_smem = 0;
-    void (*bulk_kernel)(Bsr<V>, BulkPlan, const X*, X*, const unsigned char*, CgScalars*,
-                        double*) = nullptr;
 
     int setup() {
         RB = reduction_blocks(c);
         if (mf) return NB2_OK;  // the Jacobi inverse comes from the matrix-free setup
         A = Bsr<V>{c->brp, c->bcol, vals, c->N};
-        bulk = make_bulk_plan(c, (int)sizeof(V), &plan);
-        const int rpw = bulk ? plan.rows_per_chunk / kBulkWarps : 0;
-        switch (rpw) {
-            case 8: bulk_kernel = k_spmv_bulk<V, X, 8>; break;
-            case 4: bulk_kernel = k_spmv_bulk<V, X, 4>; break;
-            case 2: bulk_kernel = k_spmv_bulk<V, X, 2>; break;
-            default: bulk_kernel = k_spmv_bulk<V, X, 1>; break;
-        }
-        if (bulk) {
-            bulk_smem = (size_t)kStages * (plan.stage_val_bytes + plan.stage_col_bytes);
-            NB2_CUDA(c, cudaFuncSetAttribute(bulk_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)bulk_smem));
-            const int per_sm = std::max(1, (int)((220 * 1024) / (bulk_smem + 4096)));
-            bulk_grid = std::min(plan.chunks, 148 * per_sm);
-        }
         k_invdiag<V, X><<<(c->N + 255) / 256, 256, 0, c->stream>>>(A, inv);
         c->launches++;
         return NB2_OK;
@@ -820,12 +642,8 @@ struct CgRunner {
                     continue;
                 }
             }
-            if (bulk)
-                bulk_kernel<<<bulk_grid, kRedThreads, bulk_smem, c->stream>>>(A, plan, p, q, mask,
-                                                                              c->cgs, c->partials);
-            else
-                k_spmv<V, X><<<RB, kRedThreads, 0, c->stream>>>(A, p, q, mask, c->cgs,
-                                                                c->partials);
+            k_spmv<V, X, spmv_lanes<V>()><<<RB, kRedThreads, 0, c->stream>>>(A, p, q, mask, c->cgs,
+                                                                            c->partials);
             k_xr<X><<<RB, kRedThreads, 0, c->stream>>>(n, x, r, p, q, inv, c->cgs, c->partials);
             k_p<X><<<RB, kRedThreads, 0, c->stream>>>(n, p, r, inv, c->cgs);
         }
