@@ -192,6 +192,14 @@ int nb2_save_internal_variables(nb2_ctx* ctx, int32_t converged);
  * 3x3), 1 det F [nqp], 2 plastic strain [nqp][9], 3 accumulated plastic strain [nqp]. */
 int nb2_get_quadrature_values(nb2_ctx* ctx, int32_t which, double* out);
 
+/* Quadrature values of the last update extrapolated to the nodes and averaged, the fields neon
+ * writes to its .vtu output (submesh::nodal_averaged_variable, submesh.cpp:271-344, and
+ * average_internal_variable, io/post/node_averaged_variables.hpp:18-41; extrapolation matrix
+ * of shape_function.hpp:70-100).  which = 0 Cauchy stress [num_nodes][9], 1 det F [num_nodes],
+ * 2 plastic strain [num_nodes][9], 3 accumulated plastic strain [num_nodes], 4 von Mises stress
+ * [num_nodes].  Host output. */
+int nb2_nodal_averaged_variable(nb2_ctx* ctx, int32_t which, double* out);
+
 /* static_matrix::enforce_dirichlet_conditions (static_matrix.hpp:279-320) on host CSR values
  * laid out as nb2_export_pattern: zero row and column of each listed DOF, keep the diagonal,
  * b[dof] = 0. */

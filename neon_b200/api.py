@@ -102,6 +102,7 @@ _SIGS = {
     "nb2_apply_tangent": (C.c_int, [P, P, P]),
     "nb2_apply_tangent_fp32": (C.c_int, [P, P, P]),
     "nb2_get_quadrature_values": (C.c_int, [P, C.c_int32, P]),
+    "nb2_nodal_averaged_variable": (C.c_int, [P, C.c_int32, P]),
     "nb2_apply_dirichlet": (C.c_int, [P, P, C.c_int32, P, P]),
     "nb2_pcg_solve": (C.c_int, [C.c_int32, P, P, P, P, P, C.c_double, C.c_int32,
                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
@@ -249,6 +250,16 @@ class SolidMesh:
         out = np.zeros(self.nqp * k)
         _check(lib().nb2_get_quadrature_values(self.h, idx, out.ctypes.data), self.h, which)
         return out.reshape(self.nqp, k) if k > 1 else out
+
+    NODAL = {"cauchy_stress": (0, 9), "DetF": (1, 1), "plastic_strain": (2, 9),
+             "accumulated_plastic_strain": (3, 1), "von_mises_stress": (4, 1)}
+
+    def nodal_averaged(self, which: str):
+        """A quadrature variable extrapolated to the nodes and averaged (neon's output fields)."""
+        idx, k = self.NODAL[which]
+        out = np.zeros(self.X.shape[0] * k)
+        _check(lib().nb2_nodal_averaged_variable(self.h, idx, out.ctypes.data), self.h, which)
+        return out.reshape(-1, k) if k > 1 else out
 
     def apply_dirichlet(self, dofs, K, b):
         dofs = np.ascontiguousarray(dofs, dtype=np.int32)

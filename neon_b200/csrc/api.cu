@@ -770,9 +770,14 @@ struct Newton {
         NB2_TRY(reset_status(c));
         time_begin();
         // mixed: no assembled K at all -- the stored FP64 tangent feeds the lifting, the FP64
-        // residual replacements and the FP32 matrix-free operator of the PCG
+        // residual replacements and the FP32 matrix-free operator of the PCG.  The update without
+        // assembly (at a converged displacement, or at the start of a load attempt) stores its
+        // point outputs, which the nodal averages of the file output read.
         int mode = MODE_CONSTITUTIVE | MODE_FORCE;
-        if (assemble) mode |= mixed() ? MODE_STORE : MODE_STIFFNESS;
+        if (assemble)
+            mode |= mixed() ? MODE_STORE : MODE_STIFFNESS;
+        else
+            mode |= MODE_STORE;
         NB2_TRY(launch_element_kernel(c, mode, NB2_FP64));
         t_elem += time_end();
         return read_status(c);
@@ -948,9 +953,9 @@ extern "C" int nb2_static_solve(nb2_ctx* c, const nb2_solver_options* options,
     nw.c = c;
     nw.o = *options;
     if (nw.o.linear_iterations <= 0 || nw.o.cg_maximum_iterations <= 0) return NB2_E_INPUT;
+    NB2_TRY(ensure_split_buffers(c));
     if (nw.o.precision == NB2_MIXED) {
         NB2_TRY(ensure_k32(c));
-        NB2_TRY(ensure_split_buffers(c));
         NB2_TRY(nw.alloc_mixed());
         if (!(nw.o.mixed_inner_tolerance > 0)) nw.o.mixed_inner_tolerance = 1e-4;
     } else {

@@ -32,8 +32,7 @@ constexpr int kThreads = 256;
 constexpr int kBatchChunk = 32;  // CG iterations per captured graph
 // operator / vector precision of the batched PCG
 constexpr int kModeK64 = 0;    // FP64 K, FP64 vectors
-constexpr int kModeK32V32 = 1; // FP32 K, FP32 vectors (FP64 dot products)
-constexpr int kModeK32V64 = 2; // FP32 K, FP64 vectors
+constexpr int kModeK32V64 = 1; // FP32 K, FP64 vectors (the batched mixed path)
 
 struct Tables {
     const int* row0;   // [nchunks] first block row
@@ -438,7 +437,7 @@ struct BatchState {
     int* flag_b = nullptr;
     std::vector<int> h_done, h_iters, h_status;
     std::vector<double> h_norms;
-    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
     Tables tables() const { return Tables{row0, row1, inst, first, count}; }
     Scalars scalars() const {
@@ -556,8 +555,8 @@ int batch_norms(nb2_ctx* c, BatchState* b, const double* v0, const double* v1, c
     return NB2_OK;
 }
 
-// Per-instance Jacobi-PCG on the resident K: precision NB2_FP64 (K64, FP64 vectors) or
-// NB2_MIXED (K32, FP32 vectors, FP64 dot products).  Instance i stops at its own tolerance or
+// Per-instance Jacobi-PCG on the resident K: kModeK64 (FP64 K) or kModeK32V64 (FP32 K); FP64
+// vectors and dot products in both.  Instance i stops at its own tolerance or
 // after maxit[i] iterations; an instance with b = 0 returns x = 0 at once.
 //   batch_pcg_start    Jacobi inverse, x = 0, r = b, p = D^-1 r, per-instance thresholds
 //   batch_pcg_iterate  captured blocks of iterations until every instance is done
@@ -565,26 +564,17 @@ int batch_pcg_start(nb2_ctx* c, BatchState* b, int mode, const double* rhs, doub
                     const std::vector<int>& maxit) {
     const Tables T = b->tables();
     const Scalars S = b->scalars();
-    const int nb = b->nchunks;
-    const bool f64 = mode != kModeK32V32;  // FP64 vectors
     const unsigned g = (c->N + 255) / 256;
     if (mode == kModeK64)
         k_b_invdiag<double, double><<<g, 256, 0, c->stream>>>(c->brp, c->bcol, c->K64, c->N,
                                                               c->cg_inv);
-    else if (mode == kModeK32V64)
+    else
         k_b_invdiag<float, double><<<g, 256, 0, c->stream>>>(c->brp, c->bcol, c->K32, c->N,
                                                              c->cg_inv);
-    else
-        k_b_invdiag<float, float><<<g, 256, 0, c->stream>>>(c->brp, c->bcol, c->K32, c->N,
-                                                            c->cg32_inv);
     NB2_CUDA(c, cudaMemcpyAsync(S.maxit, maxit.data(), sizeof(int) * b->ninst,
                                 cudaMemcpyHostToDevice, c->stream));
-    if (f64)
-        k_b_init<double><<<nb, kThreads, 0, c->stream>>>(T, rhs, c->cg_x, c->cg_r, c->cg_p,
-                                                          c->cg_inv, S, b->part, tol);
-    else
-        k_b_init<float><<<nb, kThreads, 0, c->stream>>>(T, rhs, c->cg32_x, c->cg32_r, c->cg32_p,
-                                                         c->cg32_inv, S, b->part, tol);
+    k_b_init<double><<<b->nchunks, kThreads, 0, c->stream>>>(T, rhs, c->cg_x, c->cg_r, c->cg_p,
+                                                              c->cg_inv, S, b->part, tol);
     c->launches += 2;
     NB2_CUDA(c, cudaStreamSynchronize(c->stream));  // maxit's host vector is the caller's
     return NB2_OK;
@@ -594,30 +584,19 @@ int batch_pcg_iterate(nb2_ctx* c, BatchState* b, int mode, int most, bool graphs
     const Tables T = b->tables();
     const Scalars S = b->scalars();
     const int nb = b->nchunks;
-    const bool f64 = mode != kModeK32V32;
     const auto spmv64 = spmv_variant<double, double>(b->lanes);
     const auto spmv3264 = spmv_variant<float, double>(b->lanes);
-    const auto spmv32 = spmv_variant<float, float>(b->lanes);
     auto enqueue = [&]() {
         for (int it = 0; it < kBatchChunk; ++it) {
-            if (f64) {
-                if (mode == kModeK64)
-                    spmv64<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K64, c->cg_p,
-                                                           c->cg_q, c->mask, S, b->part);
-                else
-                    spmv3264<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K32, c->cg_p,
-                                                             c->cg_q, c->mask, S, b->part);
-                k_b_xr<double><<<nb, kThreads, 0, c->stream>>>(T, c->cg_x, c->cg_r, c->cg_p,
-                                                               c->cg_q, c->cg_inv, S, b->part);
-                k_b_p<double><<<nb, kThreads, 0, c->stream>>>(T, c->cg_p, c->cg_r, c->cg_inv, S);
-            } else {
-                spmv32<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K32, c->cg32_p,
-                                                       c->cg32_q, c->mask, S, b->part);
-                k_b_xr<float><<<nb, kThreads, 0, c->stream>>>(T, c->cg32_x, c->cg32_r, c->cg32_p,
-                                                              c->cg32_q, c->cg32_inv, S, b->part);
-                k_b_p<float><<<nb, kThreads, 0, c->stream>>>(T, c->cg32_p, c->cg32_r, c->cg32_inv,
-                                                             S);
-            }
+            if (mode == kModeK64)
+                spmv64<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K64, c->cg_p,
+                                                       c->cg_q, c->mask, S, b->part);
+            else
+                spmv3264<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K32, c->cg_p,
+                                                         c->cg_q, c->mask, S, b->part);
+            k_b_xr<double><<<nb, kThreads, 0, c->stream>>>(T, c->cg_x, c->cg_r, c->cg_p, c->cg_q,
+                                                           c->cg_inv, S, b->part);
+            k_b_p<double><<<nb, kThreads, 0, c->stream>>>(T, c->cg_p, c->cg_r, c->cg_inv, S);
         }
     };
     cudaGraphExec_t& g = b->graph[mode];
@@ -666,10 +645,7 @@ int batch_pcg(nb2_ctx* c, BatchState* b, int mode, const double* rhs, double* xo
     NB2_TRY(batch_pcg_start(c, b, mode, rhs, tol, maxit));
     NB2_TRY(batch_pcg_iterate(c, b, mode, *std::max_element(maxit.begin(), maxit.end()),
                               graphs));
-    if (mode != kModeK32V32)
-        k_b_out<double><<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->cg_x, xout);
-    else
-        k_b_out<float><<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->cg32_x, xout);
+    k_b_out<double><<<vgrid(c->n), 256, 0, c->stream>>>(c->n, c->cg_x, xout);
     c->launches++;
     NB2_CUDA(c, cudaGetLastError());
     return NB2_OK;

@@ -64,6 +64,7 @@ def lib():
         L.orc_save.argtypes = [P, C.c_int]
         L.orc_get_qp.argtypes = [P, C.c_int, dp]
         L.orc_set_qp.argtypes = [P, C.c_int, dp]
+        L.orc_nodal_average.argtypes = [P, C.c_int, dp]
         L.orc_constitutive_only.argtypes = [P]
         L.orc_cg_solve.argtypes = [C.c_int, ip, ip, dp, dp, dp, C.c_double, C.c_int, C.c_int,
                                    C.POINTER(C.c_int), C.POINTER(C.c_double)]
@@ -184,6 +185,16 @@ class OracleMesh:
         out = np.zeros(self.E * self.nq * k)
         lib().orc_get_qp(self.h, which, out)
         return out.reshape(self.E * self.nq, k) if k > 1 else out
+
+    # submesh::nodal_averaged_variable + average_internal_variable (value / count per node)
+    NODAL = {"cauchy_stress": (0, 9), "DetF": (1, 1), "plastic_strain": (2, 9),
+             "accumulated_plastic_strain": (3, 1), "von_mises_stress": (4, 1)}
+
+    def nodal_average(self, name):
+        which, k = self.NODAL[name]
+        out = np.zeros(self.N * k)
+        lib().orc_nodal_average(self.h, which, out)
+        return out.reshape(self.N, k) if k > 1 else out
 
     def set(self, name, values):
         which, _ = QP[name]

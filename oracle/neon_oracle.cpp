@@ -1507,4 +1507,81 @@ int orc_static_solve(void* h, const orc_options* opt, int nbc, const int* bc_dof
     return st;
 }
 
+// shape_function::compute_extrapolation_matrix (interpolations/shape_function.hpp:70-100) for the
+// two element types of the path.  hex8 with its 8 points: m == n, E = N^-1 where row l of N holds
+// the hexahedron8 shape functions at point l (hexahedron.cpp:10-67, corner and point order as in
+// make_hex8); inverted by Gauss-Jordan elimination with partial pivoting.  tet4 with one point:
+// E = ones(4, 1) (tetrahedron.cpp:38-43).  E is [npe][nq].
+static std::vector<double> extrapolation_matrix(int npe) {
+    if (npe == 4) return {1.0, 1.0, 1.0, 1.0};
+    const double lc[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                             {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+    const double g = 1.0 / std::sqrt(3.0);
+    double A[8][16];
+    for (int l = 0; l < 8; ++l) {
+        for (int a = 0; a < 8; ++a)
+            A[l][a] = 0.125 * (1.0 + lc[a][0] * g * lc[l][0]) * (1.0 + lc[a][1] * g * lc[l][1]) *
+                      (1.0 + lc[a][2] * g * lc[l][2]);
+        for (int a = 0; a < 8; ++a) A[l][8 + a] = (l == a) ? 1.0 : 0.0;
+    }
+    for (int c = 0; c < 8; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 8; ++r)
+            if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
+        for (int k = 0; k < 16; ++k) std::swap(A[c][k], A[piv][k]);
+        const double d = A[c][c];
+        for (int k = 0; k < 16; ++k) A[c][k] /= d;
+        for (int r = 0; r < 8; ++r) {
+            if (r == c) continue;
+            const double f = A[r][c];
+            for (int k = 0; k < 16; ++k) A[r][k] -= f * A[c][k];
+        }
+    }
+    std::vector<double> E(64);  // E[a][l] = (N^-1)[a][l]
+    for (int a = 0; a < 8; ++a)
+        for (int l = 0; l < 8; ++l) E[a * 8 + l] = A[a][8 + l];
+    return E;
+}
+
+// submesh::nodal_averaged_variable (mesh/mechanics/solid/submesh.cpp:271-344) followed by
+// average_internal_variable (io/post/node_averaged_variables.hpp:18-41): element by element the
+// point values of each component are extrapolated with E and added to the element's nodes,
+// each addition counted; the nodal value is the sum over the count.
+// which: 0 Cauchy stress [N][9], 1 det F [N], 2 plastic strain [N][9],
+//        3 accumulated plastic strain [N], 4 von Mises stress [N]
+int orc_nodal_average(void* h, int which, double* out) {
+    auto* o = static_cast<Oracle*>(h);
+    const std::vector<double>* v = nullptr;
+    int nc = 1;
+    switch (which) {
+        case 0: v = &o->sigma; nc = 9; break;
+        case 1: v = &o->detF; break;
+        case 2: v = &o->ep; nc = 9; break;
+        case 3: v = &o->epbar; break;
+        case 4: v = &o->vm; break;
+        default: return 1;
+    }
+    const std::vector<double> E = extrapolation_matrix(o->npe);
+    std::vector<double> value((size_t)o->N * nc, 0.0), count((size_t)o->N * nc, 0.0);
+    const int nq = o->nq, npe = o->npe;
+    std::vector<double> comp(nq);
+    for (int e = 0; e < o->E; ++e) {
+        const int* nodes = &o->conn[(size_t)e * npe];
+        for (int c = 0; c < nc; ++c) {
+            for (int l = 0; l < nq; ++l) {
+                const size_t q = (size_t)e * nq + l;
+                comp[l] = v->empty() ? 0.0 : (*v)[q * nc + c];
+            }
+            for (int a = 0; a < npe; ++a) {
+                double t = 0.0;
+                for (int l = 0; l < nq; ++l) t += E[a * nq + l] * comp[l];
+                value[(size_t)nodes[a] * nc + c] += t;
+                count[(size_t)nodes[a] * nc + c] += 1.0;
+            }
+        }
+    }
+    for (size_t i = 0; i < value.size(); ++i) out[i] = value[i] / count[i];
+    return 0;
+}
+
 }  // extern "C"
