@@ -114,7 +114,7 @@ static int dev_alloc(nb2_ctx* c, T** p, long long count) {
 int nb2::ensure_split_buffers(nb2_ctx* c) {
     if (c->sig) return NB2_OK;
     NB2_TRY(dev_alloc(c, &c->sig, 6ll * c->nqp));
-    NB2_TRY(dev_alloc(c, &c->dpar, 9ll * c->nqp));
+    NB2_TRY(dev_alloc(c, &c->dpar, (long long)dpar_rows(c->mat.model) * c->nqp));
     NB2_TRY(dev_alloc(c, &c->detF, (long long)c->nqp));
     NB2_TRY(dev_alloc(c, &c->u_tan, (long long)c->n));
     return NB2_OK;
@@ -143,7 +143,7 @@ int nb2_create(const nb2_mesh_desc* m, const nb2_material* mat, nb2_ctx** out) {
     *out = nullptr;
     if (!m || !mat || !m->coordinates || !m->connectivity || m->num_nodes <= 0 ||
         m->num_elements <= 0 || (m->nodes_per_element != 8 && m->nodes_per_element != 4) ||
-        mat->model < 0 || mat->model > 3) {
+        mat->model < 0 || mat->model > 4) {
         g_create_error = "invalid mesh or material description";
         return NB2_E_INPUT;
     }

@@ -8,22 +8,25 @@
 //   phase 2  each lane accumulates its upper-triangular 3x3 blocks over the points in Real
 //            precision, in two passes of at most 3 blocks (fewer live registers), and adds
 //            them (and their mirrored blocks) to K with red.global.add.
-// Shared memory per element holds L (Real) for every point, the flow direction N (J2) and,
-// for finite-strain models, g = s sigma L (FP64) used by the geometric stiffness.
+// Shared memory per element holds L (Real) for every point, the flow direction N (J2) or the
+// anisotropic tangent s Da (Langevin microsphere) and, for finite-strain models, g = s sigma L
+// (FP64) used by the geometric stiffness.
 #pragma once
 
 template <int NPE, int MODEL, typename Real, int MODE>
-__global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : 8) k_element(ElementArgs A) {
+__global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : ((MODEL == MODEL_ML) ? 4 : 8))
+    k_element(ElementArgs A) {
     using T = Topo<NPE>;
     constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC, MAXB = T::MAXB;
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || MODEL == MODEL_ML);
     constexpr bool kJ2 = (MODEL == MODEL_J2);
+    constexpr bool kAniso = (MODEL == MODEL_ML);
     constexpr bool kCon = (MODE & MODE_CONSTITUTIVE) != 0;
     constexpr bool kStiff = (MODE & MODE_STIFFNESS) != 0;
     constexpr bool kForce = (MODE & MODE_FORCE) != 0;
     constexpr bool kStore = (MODE & MODE_STORE) != 0;
     constexpr int LS = NQ * NPE * 3 + 2;           // per-element stride of L (padded)
-    constexpr int NS = kJ2 ? NQ * 6 + 2 : 1;       // flow directions
+    constexpr int NS = kJ2 ? NQ * 6 + 2 : (kAniso ? NQ * 21 + 2 : 1);  // N or s Da
     constexpr int GS = kFinite ? NQ * NPE * 3 + 1 : 1;  // g = s sigma L
     constexpr int NG = (NPE + G - 1) / G;          // nodes per lane
 
@@ -121,8 +124,10 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : 8) k_element(Ele
                     cm_neo_hooke(Ae, Fd, detF, o);
                 } else if constexpr (MODEL == MODEL_J2) {
                     if (!cm_j2(A, q, Hm, o)) report_status(A, e, NB2_E_RETURN_MAP);
-                } else {
+                } else if constexpr (MODEL == MODEL_MS) {
                     cm_microsphere(Ae, Ae.G, Fd, detF, o);
+                } else {
+                    cm_langevin(Ae, Ae.G, Fd, detF, o);
                 }
                 bool bad = isnan(o.lam) || isnan(o.mu);
 #pragma unroll
@@ -135,8 +140,13 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : 8) k_element(Ele
                     A.dpar[0 * n + q] = o.lam;
                     A.dpar[1 * n + q] = o.mu;
                     A.dpar[2 * n + q] = o.b;
+                    if constexpr (kAniso) {
 #pragma unroll
-                    for (int c = 0; c < 6; ++c) A.dpar[(3 + c) * n + q] = kJ2 ? o.N[c] : 0.0;
+                        for (int c = 0; c < 21; ++c) A.dpar[(3 + c) * n + q] = o.Da[c];
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) A.dpar[(3 + c) * n + q] = kJ2 ? o.N[c] : 0.0;
+                    }
                     A.detF[q] = detF;
                 }
             } else {
@@ -146,8 +156,13 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : 8) k_element(Ele
                 o.lam = A.dpar[0 * n + q];
                 o.mu = A.dpar[1 * n + q];
                 o.b = A.dpar[2 * n + q];
+                if constexpr (kAniso) {
 #pragma unroll
-                for (int c = 0; c < 6; ++c) o.N[c] = A.dpar[(3 + c) * n + q];
+                    for (int c = 0; c < 21; ++c) o.Da[c] = A.dpar[(3 + c) * n + q];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) o.N[c] = A.dpar[(3 + c) * n + q];
+                }
             }
             inv3(Fc, Ji);
             s = w * det3(Fc);
@@ -196,6 +211,10 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : 8) k_element(Ele
                 if constexpr (kJ2 && kStiff) {
 #pragma unroll
                     for (int c = 0; c < 6; ++c) sN[le][l * 6 + c] = (Real)o.N[c];
+                }
+                if constexpr (kAniso && kStiff) {
+#pragma unroll
+                    for (int c = 0; c < 21; ++c) sN[le][l * 21 + c] = (Real)(s * o.Da[c]);
                 }
                 sC[le][l][0] = (Real)(s * o.lam);
                 sC[le][l][1] = (Real)(s * o.mu);
@@ -291,6 +310,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : 8) k_element(Ele
                                 if (i == k) v += diag;
                                 acc[jj][3 * i + k] += v;
                             }
+                        if constexpr (kAniso) aniso_block(&sN[le][l * 21], La, Lb, acc[jj]);
                         if constexpr (kJ2) {
                             if (cb != (Real)0) {
                                 Real va[3], vb[3];

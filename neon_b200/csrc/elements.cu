@@ -27,6 +27,10 @@
 //              microsphere    D = (k+p)1(x)1 - 2p I + P Dbar P with P(tau(x)1)P = 0 and
 //                             P I P = I_dev -> lam' = k + p - 2/9 tr tau, mu' = tr tau/3 - p
 //                             (gaussian_affine_microsphere.cpp:58-74);
+//              Langevin       the same isotropic part plus the projected macro moduli
+//              microsphere    P Cbar P = sum_i c_i m_i (x) m_i (m_i = dev(t_i (x) t_i)), a
+//                             general symmetric 6x6 Da (affine_microsphere.cpp:58-112):
+//                             K_ab += s B_a^T Da B_b;
 //            the stiffness phase runs in Real (FP64 for parity, FP32 for the mixed path);
 //   phase 3  each lane adds its blocks (and the mirrored lower blocks) with red.global.add into
 //            K[slot], and the force of one node into f_int.
@@ -107,6 +111,7 @@ struct QpOut {
     double sig[6];  // Cauchy stress
     double lam, mu, b;
     double N[6];    // J2 flow direction (plastic points)
+    double Da[21];  // Langevin microsphere: anisotropic tangent, packed upper triangle (sym6)
 };
 
 // ----- constitutive models (FP64) --------------------------------------------------------
@@ -247,6 +252,108 @@ __device__ __forceinline__ void cm_microsphere(const ElementArgs& A, double Gm, 
     o.b = 0.0;
 }
 
+// affine_microsphere.cpp:23-112 with the Pade approximants of detail/microsphere.hpp:40-70.
+// Per sphere direction r_i: t = Fbar r_i, l^2 = t.t, d = N - l^2,
+//   pade_first  = (3N - l^2) / d,   pade_second = (l^4 + 3N^2) / d^2,
+//   tau    = G sum_i w_i pade_first t (x) t,
+//   Cbar   = G sum_i w_i l^-2 (pade_second - pade_first) t(x)t(x)t(x)t.
+// The tangent (k + p) 1(x)1 - 2p I + P (Cbar + 2/3 tr tau I - 2/3 (tau(x)1 + 1(x)tau)) P splits
+// as for the Gaussian model into lam', mu' and the projected macro moduli
+//   Da = P Cbar P = G sum_i w_i l^-2 (pade_second - pade_first) m_i (x) m_i,  m_i = dev(t (x) t)
+// (P t(x)t = dev(t(x)t) in kinetic Voigt), accumulated directly as a packed 6x6.
+__device__ __forceinline__ void cm_langevin(const ElementArgs& A, double Gm, const double* F,
+                                            double J, QpOut& o) {
+    const double K = A.K, Nc = A.Nseg;
+    double sc = pow(det3(F), -1.0 / 3.0);
+    double Fb[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Fb[i] = sc * F[i];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < 21; ++c) o.Da[c] = 0.0;
+#pragma unroll 1
+    for (int i = 0; i < 21; ++i) {
+        double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1], r2 = c_sphere_r[3 * i + 2];
+        double w = c_sphere_w[i];
+        double t0 = Fb[0] * r0 + Fb[1] * r1 + Fb[2] * r2;
+        double t1 = Fb[3] * r0 + Fb[4] * r1 + Fb[5] * r2;
+        double t2 = Fb[6] * r0 + Fb[7] * r1 + Fb[8] * r2;
+        const double l2 = t0 * t0 + t1 * t1 + t2 * t2;
+        const double d = Nc - l2;
+        const double pf = (3.0 * Nc - l2) / d;
+        const double ps = (l2 * l2 + 3.0 * Nc * Nc) / (d * d);
+        const double wf = w * pf;
+        acc[0] += (t0 * t0) * wf;
+        acc[1] += (t1 * t1) * wf;
+        acc[2] += (t2 * t2) * wf;
+        acc[3] += (t1 * t2) * wf;
+        acc[4] += (t0 * t2) * wf;
+        acc[5] += (t0 * t1) * wf;
+        const double a4 = Gm * w * (ps - pf) / l2;
+        const double l3 = l2 / 3.0;
+        const double m[6] = {t0 * t0 - l3, t1 * t1 - l3, t2 * t2 - l3, t1 * t2, t0 * t2, t0 * t1};
+#pragma unroll
+        for (int v = 0; v < 6; ++v)
+#pragma unroll
+            for (int u = v; u < 6; ++u) o.Da[sym6(v, u)] += a4 * m[v] * m[u];
+    }
+    double tau[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tau[c] = Gm * acc[c];
+    double p = J * (K / 2.0 * (J - 1.0 / J));
+    double trt = tau[0] + tau[1] + tau[2];
+    double tr3 = trt / 3.0;
+    o.sig[0] = (p + tau[0] - tr3) / J;
+    o.sig[1] = (p + tau[1] - tr3) / J;
+    o.sig[2] = (p + tau[2] - tr3) / J;
+    o.sig[3] = tau[3] / J;
+    o.sig[4] = tau[4] / J;
+    o.sig[5] = tau[5] / J;
+    double kappa = (J * J) * (K / 2.0 * (1.0 + 1.0 / (J * J)));
+    o.lam = kappa + p - (2.0 / 9.0) * trt;
+    o.mu = trt / 3.0 - p;
+    o.b = 0.0;
+}
+
+// y += B_a^T Da B_b restricted to one 3x3 block: K[i][k] += sum_vw B_a[v][i] Da[v][w] B_b[w][k]
+// with the kinematic strain operator B (rows 11 22 33 23 13 12; shear rows engineering).
+// Column k of B_b has three entries: k=0 -> rows (0, 4, 5) = (L0, L2, L1), k=1 -> (1, 3, 5) =
+// (L1, L2, L0), k=2 -> (2, 3, 4) = (L2, L1, L0).
+template <typename Real, typename DaT>
+__device__ __forceinline__ void aniso_block(const DaT* Da, const Real* La, const Real* Lb,
+                                            Real* acc) {
+    Real Z[6][3];
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+        Z[v][0] = (Real)Da[sym6(v, 0)] * Lb[0] + (Real)Da[sym6(v, 4)] * Lb[2] +
+                  (Real)Da[sym6(v, 5)] * Lb[1];
+        Z[v][1] = (Real)Da[sym6(v, 1)] * Lb[1] + (Real)Da[sym6(v, 3)] * Lb[2] +
+                  (Real)Da[sym6(v, 5)] * Lb[0];
+        Z[v][2] = (Real)Da[sym6(v, 2)] * Lb[2] + (Real)Da[sym6(v, 3)] * Lb[1] +
+                  (Real)Da[sym6(v, 4)] * Lb[0];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        acc[0 * 3 + k] += La[0] * Z[0][k] + La[2] * Z[4][k] + La[1] * Z[5][k];
+        acc[1 * 3 + k] += La[1] * Z[1][k] + La[2] * Z[3][k] + La[0] * Z[5][k];
+        acc[2 * 3 + k] += La[2] * Z[2][k] + La[1] * Z[3][k] + La[0] * Z[4][k];
+    }
+}
+
+// sigma_a = Da eps with eps the engineering strain of the gradient G (row-major 3x3); returns
+// the symmetric stress in kinetic Voigt order
+template <typename Real, typename DaT>
+__device__ __forceinline__ void aniso_stress(const DaT* Da, const Real* G, Real* sa) {
+    const Real eps[6] = {G[0], G[4], G[8], G[5] + G[7], G[2] + G[6], G[1] + G[3]};
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+        Real t = (Real)0;
+#pragma unroll
+        for (int w = 0; w < 6; ++w) t += (Real)Da[sym6(v, w)] * eps[w];
+        sa[v] = t;
+    }
+}
+
 // The material moduli of element e: per-element shear / bulk modulus when given (batched
 // instances of different materials, per-element parameter fields), else the material's.
 __device__ __forceinline__ ElementArgs element_moduli(const ElementArgs& A, long long e) {
@@ -275,7 +382,7 @@ __device__ __forceinline__ bool element_enabled(const ElementArgs& A, long long 
 // Matrix-free FP64 product y += K v with the tangent of the last stored update: the defect
 // residual of the mixed-precision solve.  With G = sum_b v_b (x) L_b (the gradient of v) the
 // element force of node a is
-//   y_a = s [lam' tr(G) La + mu' (G + G^T) La + b (N:G) N La + G sigma La]
+//   y_a = s [lam' tr(G) La + mu' (G + G^T) La + b (N:G) N La + (Da eps(G)) La + G sigma La]
 // -- the same tangent the assembled K holds, applied without forming it.
 // ---------------------------------------------------------------------------------------
 template <int NPE, int MODEL>
@@ -283,8 +390,9 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
                                               double* __restrict__ y) {
     using T = Topo<NPE>;
     constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC;
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || MODEL == MODEL_ML);
     constexpr bool kJ2 = (MODEL == MODEL_J2);
+    constexpr bool kAniso = (MODEL == MODEL_ML);
     __shared__ double sx[EPC][NPE][3];
     __shared__ double sv[EPC][NPE][3];
     __shared__ double sdN[NQ][NPE][3];
@@ -354,6 +462,13 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
                           N6[5] * (Gm[1] + Gm[3]));
             }
         }
+        double sa[6] = {0, 0, 0, 0, 0, 0};
+        if constexpr (kAniso) {
+            double Da[21];
+#pragma unroll
+            for (int c = 0; c < 21; ++c) Da[c] = A.dpar[(3 + c) * n + q];
+            aniso_stress(Da, Gm, sa);
+        }
         double sg[6] = {0, 0, 0, 0, 0, 0};
         if constexpr (kFinite) {
 #pragma unroll
@@ -373,6 +488,11 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
                 t[0] += bN * (N6[0] * La[0] + N6[5] * La[1] + N6[4] * La[2]);
                 t[1] += bN * (N6[5] * La[0] + N6[1] * La[1] + N6[3] * La[2]);
                 t[2] += bN * (N6[4] * La[0] + N6[3] * La[1] + N6[2] * La[2]);
+            }
+            if constexpr (kAniso) {
+                t[0] += sa[0] * La[0] + sa[5] * La[1] + sa[4] * La[2];
+                t[1] += sa[5] * La[0] + sa[1] * La[1] + sa[3] * La[2];
+                t[2] += sa[4] * La[0] + sa[3] * La[1] + sa[2] * La[2];
             }
             if constexpr (kFinite) {
                 const double sl0 = sg[0] * La[0] + sg[5] * La[1] + sg[4] * La[2];
@@ -807,6 +927,7 @@ static int dispatch_model(nb2_ctx* c, const ElementArgs& A, int mode, int precis
         case MODEL_NH: return dispatch_mode<NPE, MODEL_NH>(c, A, mode, precision);
         case MODEL_J2: return dispatch_mode<NPE, MODEL_J2>(c, A, mode, precision);
         case MODEL_MS: return dispatch_mode<NPE, MODEL_MS>(c, A, mode, precision);
+        case MODEL_ML: return dispatch_mode<NPE, MODEL_ML>(c, A, mode, precision);
     }
     return NB2_E_INPUT;
 }
@@ -821,6 +942,7 @@ static void launch_apply_t(nb2_ctx* c, const ElementArgs& A, const double* v, do
         case MODEL_LE: k_apply<NPE, MODEL_LE><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         case MODEL_NH: k_apply<NPE, MODEL_NH><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         case MODEL_J2: k_apply<NPE, MODEL_J2><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+        case MODEL_ML: k_apply<NPE, MODEL_ML><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         default: k_apply<NPE, MODEL_MS><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
     }
     c->launches++;
@@ -863,6 +985,7 @@ int launch_mf_setup(nb2_ctx* c) {
         case MODEL_LE: hex ? mf_setup_t<8, MODEL_LE>(c, A) : mf_setup_t<4, MODEL_LE>(c, A); break;
         case MODEL_NH: hex ? mf_setup_t<8, MODEL_NH>(c, A) : mf_setup_t<4, MODEL_NH>(c, A); break;
         case MODEL_J2: hex ? mf_setup_t<8, MODEL_J2>(c, A) : mf_setup_t<4, MODEL_J2>(c, A); break;
+        case MODEL_ML: hex ? mf_setup_t<8, MODEL_ML>(c, A) : mf_setup_t<4, MODEL_ML>(c, A); break;
         default: hex ? mf_setup_t<8, MODEL_MS>(c, A) : mf_setup_t<4, MODEL_MS>(c, A); break;
     }
     NB2_CUDA(c, cudaGetLastError());
@@ -874,6 +997,7 @@ int mf_coefficients(int model) {
         case MODEL_LE: return MfCoef<MODEL_LE>::KC;
         case MODEL_NH: return MfCoef<MODEL_NH>::KC;
         case MODEL_J2: return MfCoef<MODEL_J2>::KC;
+        case MODEL_ML: return MfCoef<MODEL_ML>::KC;
         default: return MfCoef<MODEL_MS>::KC;
     }
 }
@@ -892,6 +1016,7 @@ void enqueue_apply32(nb2_ctx* c, const float* v, float* ye, const int* done) {
         case MODEL_LE: hex ? apply32_t<8, MODEL_LE>(c, v, ye, done) : apply32_t<4, MODEL_LE>(c, v, ye, done); break;
         case MODEL_NH: hex ? apply32_t<8, MODEL_NH>(c, v, ye, done) : apply32_t<4, MODEL_NH>(c, v, ye, done); break;
         case MODEL_J2: hex ? apply32_t<8, MODEL_J2>(c, v, ye, done) : apply32_t<4, MODEL_J2>(c, v, ye, done); break;
+        case MODEL_ML: hex ? apply32_t<8, MODEL_ML>(c, v, ye, done) : apply32_t<4, MODEL_ML>(c, v, ye, done); break;
         default: hex ? apply32_t<8, MODEL_MS>(c, v, ye, done) : apply32_t<4, MODEL_MS>(c, v, ye, done); break;
     }
 }
@@ -904,7 +1029,7 @@ static int launch_jvp_t(nb2_ctx* c, const ElementArgs& A, const double* v, doubl
         case MODEL_LE: k_force_jvp<NPE, MODEL_LE><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         case MODEL_NH: k_force_jvp<NPE, MODEL_NH><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         case MODEL_MS: k_force_jvp<NPE, MODEL_MS><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
-        default: return NB2_E_INPUT;  // J2 carries history: no exact tangent product here
+        default: return NB2_E_INPUT;  // J2 carries history; no Langevin product here
     }
     c->launches++;
     return NB2_OK;
@@ -951,6 +1076,7 @@ static ElementArgs make_args(nb2_ctx* c) {
     A.lambda = c->mat.bulk_modulus - 2.0 * c->mat.shear_modulus / 3.0;
     A.sigma_y = c->mat.yield_stress;
     A.H_iso = c->mat.isotropic_hardening_modulus;
+    A.Nseg = c->mat.segments_per_chain;
     A.Ge = c->Ge;
     A.Ke = c->Ke;
     A.ep = c->ep;
@@ -993,15 +1119,17 @@ int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
 
 // Canonical algorithmic FLOPs per element (hex8 small strain 29,040; hex8 finite strain 32,240;
 // tet4 finite strain 1,552) plus the constitutive update per point (LE 60, NH 120, J2 250,
-// microsphere BO21 2,000).
+// microsphere BO21 2,000, Langevin microsphere BO21 3,000); the Langevin anisotropic tangent
+// adds 81 FMAs per block and point (hex8 36 blocks x 8 points, tet4 10 x 1).
 void element_flop_model(const nb2_ctx* c, double* flops_per_element) {
     double base;
-    bool finite = c->mat.model == MODEL_NH || c->mat.model == MODEL_MS;
+    bool finite = c->mat.model == MODEL_NH || c->mat.model == MODEL_MS || c->mat.model == MODEL_ML;
     if (c->npe == 8)
         base = finite ? 32240.0 : 29040.0;
     else
         base = 1552.0;
-    const double cm[4] = {60.0, 120.0, 250.0, 2000.0};
+    if (c->mat.model == MODEL_ML) base += 2.0 * 81.0 * (c->npe == 8 ? 36 * 8 : 10);
+    const double cm[5] = {60.0, 120.0, 250.0, 2000.0, 3000.0};
     *flops_per_element = base + c->nq * cm[c->mat.model];
 }
 

@@ -5,14 +5,15 @@
 // The same operator applied element by element needs far less: per element the FP32 node
 // coordinates relative to its first node (96 B; differences taken in FP64, so no cancellation
 // in FP32), per quadrature point the tangent coefficients pre-multiplied by w det J (2 floats;
-// J2 plastic points 9, finite strain 8), the node indices, and the input/output vectors.
+// J2 plastic points 9, finite strain 8, Langevin microsphere 8 + 21), the node indices, and the
+// input/output vectors.
 //   k_mf_setup  once per linear solve (after an element pass that stored its outputs): writes
 //               those FP32 data and each element's contribution to diag(K) (Jacobi);
 //   k_apply32   per CG iteration: y_e = K_e v_e in FP32, written per element (ye[E][npe*3]);
 //               a node-ordered gather (pcg.cu) sums ye into q without atomics, in a fixed order.
 // With G = sum_b v_b (x) L_b the element force of node a is (the product the assembled blocks
 //   K_ab = s[lam' La(x)Lb + mu'((La.Lb) I + Lb(x)La) + b (N La)(x)(N Lb)] + s (La.sigma.Lb) I
-// give) y_a = s [lam' tr(G) La + mu' (G + G^T) La + b (N:G) N La + G sigma La].
+// give) y_a = s [lam' tr(G) La + mu' (G + G^T) La + b (N:G) N La + (Da eps(G)) La + G sigma La].
 #pragma once
 
 __device__ __forceinline__ float det3f(const float* m) {
@@ -39,20 +40,23 @@ __device__ __forceinline__ void inv3f(const float* m, float* r) {
 // number of FP32 coefficients per quadrature point
 template <int MODEL>
 struct MfCoef {
-    static constexpr int KC = (MODEL == MODEL_J2) ? 9 : ((MODEL == MODEL_LE) ? 2 : 8);
+    static constexpr int KC =
+        (MODEL == MODEL_J2) ? 9 : ((MODEL == MODEL_LE) ? 2 : ((MODEL == MODEL_ML) ? 8 + 21 : 8));
 };
 
 // Setup from the stored FP64 outputs of the last MODE_STORE pass (A.u = its displacement):
 //   md[e][3a+k]  = (float)(x_a - x_0)_k
 //   mc[c][q]     = s lam', s mu' | J2: s b, N (6) | finite strain: s sigma (6)
+//                  | Langevin microsphere: then s Da (21, packed upper triangle)
 //   de[e][3a+i]  = element contribution to K_(3a+i, 3a+i)
 template <int NPE, int MODEL>
 __global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restrict__ md,
                                                  float* __restrict__ mc, float* __restrict__ de) {
     using T = Topo<NPE>;
     constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC;
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || MODEL == MODEL_ML);
     constexpr bool kJ2 = (MODEL == MODEL_J2);
+    constexpr bool kAniso = (MODEL == MODEL_ML);
     __shared__ double sx[EPC][NPE][3];
     __shared__ double sdN[NQ][NPE][3];
     __shared__ double sD[EPC][NQ][NPE * 3];
@@ -116,6 +120,14 @@ __global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restric
                 mc[(2 + c) * n + q] = (float)(s * sg[c]);
             }
         }
+        double Da[kAniso ? 21 : 1];
+        if constexpr (kAniso) {
+#pragma unroll
+            for (int c = 0; c < 21; ++c) {
+                Da[c] = A.dpar[(3 + c) * n + q];
+                mc[(8 + c) * n + q] = (float)(s * Da[c]);
+            }
+        }
 #pragma unroll
         for (int a = 0; a < NPE; ++a) {
             double La[3];
@@ -134,10 +146,12 @@ __global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restric
             if constexpr (kFinite)
                 geo = sg[0] * La[0] * La[0] + sg[1] * La[1] * La[1] + sg[2] * La[2] * La[2] +
                       2.0 * (sg[3] * La[1] * La[2] + sg[4] * La[0] * La[2] + sg[5] * La[0] * La[1]);
+            double ka[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            if constexpr (kAniso) aniso_block(Da, La, La, ka);
 #pragma unroll
             for (int i = 0; i < 3; ++i)
-                sD[le][l][3 * a + i] =
-                    s * (lam * La[i] * La[i] + mu * (LL + La[i] * La[i]) + b * nl[i] * nl[i] + geo);
+                sD[le][l][3 * a + i] = s * (lam * La[i] * La[i] + mu * (LL + La[i] * La[i]) +
+                                            b * nl[i] * nl[i] + geo + ka[4 * i]);
         }
     }
     __syncthreads();
@@ -182,7 +196,7 @@ template <int MODEL>
 __device__ __forceinline__ void point_flux(const float* J, const float* Gx,
                                            const float* __restrict__ mc, long long nqp,
                                            long long q, float* Pm) {
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS);
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || MODEL == MODEL_ML);
     constexpr bool kJ2 = (MODEL == MODEL_J2);
     float Ji[9];
     inv3f(J, Ji);
@@ -216,6 +230,16 @@ __device__ __forceinline__ void point_flux(const float* J, const float* Gx,
             S[2] += bN * N6[4]; S[6] += bN * N6[4];
             S[1] += bN * N6[5]; S[3] += bN * N6[5];
         }
+    }
+    if constexpr (MODEL == MODEL_ML) {
+        float Da[21], sa[6];
+#pragma unroll
+        for (int c = 0; c < 21; ++c) Da[c] = mc[(8 + c) * nqp + q];
+        aniso_stress(Da, G, sa);
+        S[0] += sa[0]; S[4] += sa[1]; S[8] += sa[2];
+        S[5] += sa[3]; S[7] += sa[3];
+        S[2] += sa[4]; S[6] += sa[4];
+        S[1] += sa[5]; S[3] += sa[5];
     }
     if constexpr (kFinite) {
         float sg[9];

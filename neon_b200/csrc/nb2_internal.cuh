@@ -20,10 +20,22 @@ namespace nb2 {
 //   values       K[nnzb][9]        (row-major 3x3 block, FP64 or FP32)
 //   slot map     slot[E][npe*npe]  (block index of element block (a,b))
 //   qp state     SoA: ep[6][nqp], epbar[nqp] (current) and their committed copies
-//   qp outputs   sig[6][nqp], dpar[9][nqp], detF[nqp] (only for the split update/assemble path)
+//   qp outputs   sig[6][nqp], dpar[rows][nqp], detF[nqp] (only for the split update/assemble
+//                path); dpar rows: lam', mu', b, then the J2 flow direction N (6) or, for the
+//                Langevin microsphere, the anisotropic tangent (21, packed upper triangle)
 // ---------------------------------------------------------------------------------------
 
-enum : int { MODEL_LE = 0, MODEL_NH = 1, MODEL_J2 = 2, MODEL_MS = 3 };
+// MODEL_MS: Gaussian affine microsphere, MODEL_ML: Langevin affine microsphere
+enum : int { MODEL_LE = 0, MODEL_NH = 1, MODEL_J2 = 2, MODEL_MS = 3, MODEL_ML = 4 };
+
+// rows of dpar for a model
+inline int dpar_rows(int model) { return model == MODEL_ML ? 3 + 21 : 9; }
+
+// Packed index of the symmetric 6x6 (kinetic Voigt 11 22 33 23 13 12) entry (v, w): the upper
+// triangle row by row.
+__host__ __device__ constexpr int sym6(int v, int w) {
+    return v <= w ? v * 6 - v * (v - 1) / 2 + (w - v) : w * 6 - w * (w - 1) / 2 + (v - w);
+}
 
 // element-kernel mode bits
 enum : int {
@@ -47,6 +59,7 @@ struct ElementArgs {
     int E;
     int nqp;
     double K, G, lambda, sigma_y, H_iso;
+    double Nseg;       // segments per chain (Langevin microsphere)
     const double* Ge;  // per-element shear modulus (or null)
     const double* Ke;  // per-element bulk modulus (or null)
     double* ep;      // [6][nqp]
@@ -55,7 +68,7 @@ struct ElementArgs {
     float* K32;
     double* fint;    // [3N]
     double* sig;     // [6][nqp]
-    double* dpar;    // [9][nqp]
+    double* dpar;    // [dpar_rows(model)][nqp]
     double* detF;    // [nqp]
     DeviceStatus* status;
     // batched instances (all null outside a batched solve): element -> instance, the instances

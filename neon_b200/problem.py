@@ -15,12 +15,14 @@ from .mesh import Mesh, quad4_consistent_forces, structured_hex8, structured_tet
 
 # Model identifiers of the C-ABI (include/neon_b200.h, enum nb2_model)
 LINEAR_ELASTIC, NEO_HOOKE, J2_SMALL_STRAIN, GAUSS_AFFINE_MICROSPHERE = 0, 1, 2, 3
+LANGEVIN_AFFINE_MICROSPHERE = 4
 
 MODEL_NAMES = {
     LINEAR_ELASTIC: "isotropic_linear_elasticity",
     NEO_HOOKE: "neohooke",
     J2_SMALL_STRAIN: "J2_plasticity",
     GAUSS_AFFINE_MICROSPHERE: "microsphere",
+    LANGEVIN_AFFINE_MICROSPHERE: "microsphere",
 }
 
 
@@ -46,12 +48,35 @@ class Material:
                          self.segments_per_chain], dtype=np.float64)
 
 
+def _check_microsphere_options(constitutive: dict):
+    """The microsphere branch of make_constitutive_model (constitutive_model_factory.cpp:48-120):
+    type and quadrature present and known, then the chain statistics of the affine model."""
+    for key, msg in (("type", 'Missing "type" as "affine" or "nonaffine" in microsphere model'),
+                     ("quadrature", 'Missing "quadrature" as "BO21", "BO33" or "FM900" in '
+                                    'microsphere model')):
+        if key not in constitutive:
+            raise ValueError(msg)
+    if constitutive["quadrature"] not in ("BO21", "BO33", "FM900"):
+        raise ValueError('"quadrature" field must be "BO21", "BO33" or "FM900"')
+    if constitutive["type"] == "affine":
+        if "statistics" not in constitutive:
+            raise ValueError('Missing "statistics" as "gaussian" or "langevin" in the '
+                             'microsphere model')
+        if constitutive["statistics"] not in ("gaussian", "langevin"):
+            raise ValueError('"statistics" for the microsphere model must be either '
+                             '"gaussian" or "langevin"')
+    elif constitutive["type"] != "nonaffine":
+        raise ValueError('microsphere model options are "affine" or "nonaffine"')
+
+
 def make_material(material: dict, constitutive: dict) -> Material:
     """Restates the factory make_constitutive_model (constitutive_model_factory.cpp:26-161) for the
-    four models on the path, and the parameter parsing of isotropic_elastic_property."""
+    five models on the path, and the parameter parsing of isotropic_elastic_property."""
     if "name" not in constitutive:
         raise ValueError('Missing "name" in "constitutive"')
     name = constitutive["name"]
+    if name == "microsphere":
+        _check_microsphere_options(constitutive)
     if "bulk_modulus" in material and "shear_modulus" in material:
         K, G = float(material["bulk_modulus"]), float(material["shear_modulus"])
     elif "elastic_modulus" in material and "poissons_ratio" in material:
@@ -78,18 +103,15 @@ def make_material(material: dict, constitutive: dict) -> Material:
         return Material(J2_SMALL_STRAIN, K, G, float(material["yield_stress"]),
                         float(material.get("isotropic_hardening_modulus", 0.0)))
     if name == "microsphere":
-        for key, msg in (("type", 'Missing "type" as "affine" or "nonaffine" in microsphere model'),
-                         ("quadrature", 'Missing "quadrature" as "BO21", "BO33" or "FM900" in '
-                                        'microsphere model')):
-            if key not in constitutive:
-                raise ValueError(msg)
-        if constitutive["type"] != "affine" or constitutive.get("statistics") != "gaussian" \
-                or constitutive["quadrature"] != "BO21" or "ageing" in constitutive:
-            raise NotImplementedError("only the Gaussian affine BO21 microsphere is on this path")
+        if constitutive["type"] != "affine" or constitutive["quadrature"] != "BO21" \
+                or ("ageing" in constitutive and constitutive["statistics"] == "gaussian"):
+            raise NotImplementedError("only the affine BO21 microsphere (Gaussian or Langevin "
+                                      "statistics) is on this path")
         if "segments_per_chain" not in material:
             raise ValueError("segments_per_chain not specified in material data")
-        return Material(GAUSS_AFFINE_MICROSPHERE, K, G,
-                        segments_per_chain=float(material["segments_per_chain"]))
+        model = GAUSS_AFFINE_MICROSPHERE if constitutive["statistics"] == "gaussian" \
+            else LANGEVIN_AFFINE_MICROSPHERE
+        return Material(model, K, G, segments_per_chain=float(material["segments_per_chain"]))
     raise ValueError(f"The model name {name} is not recognised")
 
 
@@ -230,12 +252,15 @@ def config_c3(n: int = 100, steps: int = 20, increments_per_step: int = 4) -> Pr
     return Problem("c3_j2_hex8_%d" % n, mesh, mat, dirichlet_boundaries(mesh, bcs, dt), opts)
 
 
-def config_c4(n: int = 48, seed_field: int = 7, traction: float = 0.05) -> Problem:
-    """Gaussian affine microsphere (BO21, K=100, G=1 scaled by a per-element lognormal(0, 0.3)
-    field), n^3 hex8, bottom clamped, uniform top traction in z (consistent quad4 forces)."""
+def config_c4(n: int = 48, seed_field: int = 7, traction: float = 0.05,
+              statistics: str = "gaussian", segments_per_chain: float = 50.0) -> Problem:
+    """Affine microsphere (BO21, K=100, G=1 scaled by a per-element lognormal(0, 0.3) field;
+    Gaussian chains, or Langevin chains of ``segments_per_chain`` segments), n^3 hex8, bottom
+    clamped, uniform top traction in z (consistent quad4 forces)."""
     mesh = structured_hex8(n)
-    mat = make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0, "segments_per_chain": 50},
-                        {"name": "microsphere", "type": "affine", "statistics": "gaussian",
+    mat = make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0,
+                         "segments_per_chain": segments_per_chain},
+                        {"name": "microsphere", "type": "affine", "statistics": statistics,
                          "quadrature": "BO21"})
     rng = np.random.Generator(np.random.PCG64(seed_field))
     Ge = rng.lognormal(mean=0.0, sigma=0.3, size=mesh.num_elements) * mat.G
@@ -246,7 +271,9 @@ def config_c4(n: int = 48, seed_field: int = 7, traction: float = 0.05) -> Probl
     opts = Options(residual_tolerance=1e-9, displacement_tolerance=1e-9, linear_iterations=15,
                    period=1.0, initial=1.0, minimum=1.0, maximum=1.0, adaptive=False,
                    cg_tolerance=1e-10, cg_maximum_iterations=200000)
-    return Problem("c4_microsphere_hex8_%d" % n, mesh, mat, dirichlet_boundaries(mesh, bcs), opts,
+    name = "c4_microsphere_hex8_%d" % n if statistics == "gaussian" else \
+        "c4_%s_microsphere_hex8_%d" % (statistics, n)
+    return Problem(name, mesh, mat, dirichlet_boundaries(mesh, bcs), opts,
                    nodal_forces=nf, element_shear_modulus=Ge)
 
 

@@ -70,7 +70,13 @@ enum : int {
     ORC_E_CUTBACK_LIMIT = 10,
 };
 
-enum : int { LINEAR_ELASTIC = 0, NEO_HOOKE = 1, J2_SMALL_STRAIN = 2, GAUSS_AFFINE_MICROSPHERE = 3 };
+enum : int {
+    LINEAR_ELASTIC = 0,
+    NEO_HOOKE = 1,
+    J2_SMALL_STRAIN = 2,
+    GAUSS_AFFINE_MICROSPHERE = 3,
+    LANGEVIN_AFFINE_MICROSPHERE = 4
+};
 
 // ----------------------------------------------------------------------------------------
 // 3x3 helpers, row-major double[9]
@@ -415,8 +421,19 @@ int update_j2(Oracle& o, size_t q) {
 }
 
 // gaussian_affine_microsphere.cpp:23-88, volumetric_free_energy.hpp:16-30,
-// detail/microsphere.hpp:16-20, tensor_operations.hpp:70-73 (unimodular)
-void update_microsphere(Oracle& o, size_t q, double G) {
+// detail/microsphere.hpp:16-20, tensor_operations.hpp:70-73 (unimodular).
+// langevin: affine_microsphere.cpp:23-112 -- the chain force and stiffness follow the Pade
+// approximants of the inverse Langevin function (detail/microsphere.hpp:40-70):
+//   macro stress  G sum_i w_i pade_first(l_i, N) t_i (x) t_i,
+//   macro moduli  G sum_i w_i l_i^-2 (pade_second - pade_first) t_i (x) t_i (x) t_i (x) t_i,
+// with l_i = |t_i|; the Gaussian model has 3 G sum_i w_i t_i (x) t_i and zero macro moduli.
+double pade_first(double l, double N) { return (3.0 * N - std::pow(l, 2)) / (N - std::pow(l, 2)); }
+double pade_second(double l, double N) {
+    return (std::pow(l, 4) + 3.0 * std::pow(N, 2)) / std::pow(N - std::pow(l, 2), 2);
+}
+
+void update_microsphere(Oracle& o, size_t q, double G, bool langevin = false) {
+    const double Nseg = o.mat.segments;
     const double K = o.mat.K;
     const double* Fq = &o.F[q * 9];
     double J = o.detF[q];
@@ -424,18 +441,33 @@ void update_microsphere(Oracle& o, size_t q, double G) {
     double Fb[9];
     for (int i = 0; i < 9; ++i) Fb[i] = scale * Fq[i];
     double pressure = J * (K / 2.0 * (J - 1.0 / J));
-    // compute_macro_stress: 3 G sum_i w_i t_i (x) t_i, t_i = Fbar r_i
+    // compute_macro_stress: 3 G sum_i w_i t_i (x) t_i, t_i = Fbar r_i (Gaussian), or
+    // G sum_i w_i pade_first t_i (x) t_i (Langevin); compute_macro_moduli (Langevin)
     double acc[9] = {0};
+    double macroC[36] = {0};
     for (int i = 0; i < 21; ++i) {
         double t[3];
         for (int a = 0; a < 3; ++a)
             t[a] = Fb[a * 3 + 0] * o.sphere.r[i][0] + Fb[a * 3 + 1] * o.sphere.r[i][1] +
                    Fb[a * 3 + 2] * o.sphere.r[i][2];
+        double f = 1.0;
+        if (langevin) {
+            const double l = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+            f = pade_first(l, Nseg);
+            const double a4 = std::pow(l, -2) * (pade_second(l, Nseg) - pade_first(l, Nseg));
+            double tt[9], tv[6];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) tt[a * 3 + b] = t[a] * t[b];
+            kinetic_voigt(tt, tv);
+            for (int a = 0; a < 6; ++a)
+                for (int b = 0; b < 6; ++b) macroC[a * 6 + b] += (a4 * tv[a] * tv[b]) * o.sphere.w[i];
+        }
         for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) acc[a * 3 + b] += (t[a] * t[b]) * o.sphere.w[i];
+            for (int b = 0; b < 3; ++b) acc[a * 3 + b] += (f * t[a] * t[b]) * o.sphere.w[i];
     }
     double tau[9];
-    for (int i = 0; i < 9; ++i) tau[i] = 3.0 * G * acc[i];
+    for (int i = 0; i < 9; ++i) tau[i] = (langevin ? G : 3.0 * G) * acc[i];
+    for (int i = 0; i < 36; ++i) macroC[i] *= G;
     // Kirchhoff stress p I + dev(tau) -> Cauchy / J
     double dev[9];
     deviatoric3(tau, dev);
@@ -445,7 +477,7 @@ void update_microsphere(Oracle& o, size_t q, double G) {
     s[4] += pressure;
     s[8] += pressure;
     for (int i = 0; i < 9; ++i) s[i] /= J;
-    // compute_material_tangent with macro moduli zero
+    // compute_material_tangent (macro moduli zero for the Gaussian model)
     double kappa = std::pow(J, 2) * (K / 2.0 * (1.0 + 1.0 / std::pow(J, 2)));
     double tv[6];
     kinetic_voigt(tau, tv);
@@ -456,7 +488,7 @@ void update_microsphere(Oracle& o, size_t q, double G) {
     for (int i = 0; i < 6; ++i)
         for (int j = 0; j < 6; ++j) {
             double Iij = (i == j) ? Ikin[i] : 0.0;
-            Dbar[i * 6 + j] = 0.0 + 2.0 / 3.0 * trt * Iij -
+            Dbar[i * 6 + j] = macroC[i * 6 + j] + 2.0 / 3.0 * trt * Iij -
                               2.0 / 3.0 * (tv[i] * one[j] + one[i] * tv[j]);
         }
     // P = kinetic deviatoric (shear diagonal 1)
@@ -573,6 +605,11 @@ int update_internal_variables(Oracle& o, const double* u, std::string* msg) {
             for (long long q = 0; q < (long long)nqp; ++q)
                 update_microsphere(o, (size_t)q, o.shear((int)(q / o.nq)));
             break;
+        case LANGEVIN_AFFINE_MICROSPHERE:
+#pragma omp parallel for schedule(static)
+            for (long long q = 0; q < (long long)nqp; ++q)
+                update_microsphere(o, (size_t)q, o.shear((int)(q / o.nq)), true);
+            break;
     }
     if (status != ORC_OK) return status;
     // FE_INVALID check (submesh.cpp:196-207) restated as a NaN scan of the outputs
@@ -645,7 +682,8 @@ void element_stiffness(const Oracle& o, int e, double* ke) {
             }
     }
     for (int i = 0; i < nd * nd; ++i) ke[i] = kmat[i];
-    bool finite = (o.mat.model == NEO_HOOKE || o.mat.model == GAUSS_AFFINE_MICROSPHERE);
+    bool finite = (o.mat.model == NEO_HOOKE || o.mat.model == GAUSS_AFFINE_MICROSPHERE ||
+                   o.mat.model == LANGEVIN_AFFINE_MICROSPHERE);
     if (!finite) return;
     std::vector<double> kgeo(npe * npe, 0.0);
     for (int l = 0; l < nq; ++l) {
@@ -1367,6 +1405,9 @@ int orc_constitutive_only(void* h) {
                 if (update_j2(*o, q)) return ORC_E_RETURN_MAP;
                 break;
             case GAUSS_AFFINE_MICROSPHERE: update_microsphere(*o, q, o->shear((int)(q / o->nq))); break;
+            case LANGEVIN_AFFINE_MICROSPHERE:
+                update_microsphere(*o, q, o->shear((int)(q / o->nq)), true);
+                break;
         }
     }
     return ORC_OK;

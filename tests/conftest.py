@@ -41,12 +41,14 @@ def random_displacement(mesh, scale, seed):
     return scale * rng.uniform(-1.0, 1.0, size=3 * mesh.num_nodes)
 
 
-def cube_example_problem():
-    """The neo-Hookean cube example (examples/.../neohooke/cube) as a Problem."""
+def cube_example_problem(example: str = "neohooke_cube_example"):
+    """A cube example on the shared cube mesh as a Problem: the neo-Hookean one
+    (examples/.../neohooke/cube) or, with ``affine_microsphere_cube_example``, the Langevin
+    affine microsphere one (examples/.../affine_microsphere/cube)."""
     from neon_b200 import mesh as M
     from neon_b200 import problem as P
     with open(os.path.join(GOLDEN, "kats.json")) as fh:
-        sim = json.load(fh)["neohooke_cube_example"]["simulation"]
+        sim = json.load(fh)[example]["simulation"]
     data = np.load(os.path.join(GOLDEN, "neohooke_cube.npz"))
     faces = {k[6:]: data[k] for k in data.files if k.startswith("group_") and k != "group_cube"}
     mesh = M.Mesh(X=data["X"], conn=M.convert_from_gmsh(data["group_cube"],
@@ -63,4 +65,4 @@ def cube_example_problem():
                      period=step["time"]["period"], initial=inc["initial"], minimum=inc["minimum"],
                      maximum=inc["maximum"], adaptive=inc["adaptive"],
                      cg_tolerance=ls["tolerance"], cg_maximum_iterations=ls["maximum_iterations"])
-    return P.Problem("neohooke_cube_example", mesh, material, bcs, opts)
+    return P.Problem(example, mesh, material, bcs, opts)

@@ -9,7 +9,9 @@ It reads the reference's Catch2 test sources and one example input as *text* and
 * ``kats.json``            numbers the reference's unit tests assert (with file:line citations);
 * ``neohooke_cube.npz``    the example mesh examples/solid_mechanics/hyperelastic/neohooke/cube/
                            cube.mesh converted to arrays (nodes, hex8 connectivity, the four
-                           boundary groups), driven by cube.json and checked by verify.py.
+                           boundary groups), driven by cube.json and checked by verify.py; the
+                           affine microsphere cube example (Langevin statistics) uses the same
+                           mesh with its own cube.json.
 
 Nothing here runs the reference.  The test suite only reads the generated files.
 """
@@ -96,6 +98,17 @@ def main(ref: str):
         "segments_per_chain": float(re.search(r'segments_per_chain\\" : ([0-9.e+-]+)',
                                               seg).group(1)),
         "uniaxial_stretch": 1.1, "margin": 1e-5}
+    la = _find_line(lines, r'TEST_CASE\("Affine microsphere"\)')
+    seg = "\n".join(lines[la:la + 85])
+    assert '\\"statistics\\":\\"langevin\\"' in seg
+    out["langevin_affine_microsphere"] = {
+        "source": f"test/hyperelastic_constitutive.cpp:{la}-{la + 83}",
+        "E": float(re.search(r'elastic_modulus\\" : ([0-9.e+-]+)', seg).group(1)),
+        "nu": float(re.search(r'poissons_ratio\\" : ([0-9.e+-]+)', seg).group(1)),
+        "segments_per_chain": float(re.search(r'segments_per_chain\\" : ([0-9.e+-]+)',
+                                              seg).group(1)),
+        "uniaxial_stretch": float(re.search(r"F\(0, 0\) = ([0-9.]+);", seg).group(1)),
+        "margin": 1e-5}
     # --- linear solver (test/linear_solvers.cpp) --------------------------------------------
     p = os.path.join(ref, "test", "linear_solvers.cpp")
     src = open(p).read()
@@ -145,6 +158,17 @@ def main(ref: str):
                   f"verify.py:{_find_line(vsrc, 'max_displacement|max\\(\\[max')}-"
                   f"{_find_line(vsrc, 'displacement gradient is incorrect')}",
         "simulation": sim, "max_displacement": 0.5, "slope": 0.5, "rel_tol": 1e-7}
+    # --- Langevin affine microsphere cube example (examples/.../affine_microsphere/cube) ----
+    # same cube.mesh as the neo-Hookean example (checked byte for byte): only the input deck
+    ax = os.path.join(ref, "examples", "solid_mechanics", "hyperelastic", "affine_microsphere",
+                      "cube")
+    with open(os.path.join(ax, "cube.mesh"), "rb") as a, open(os.path.join(ex, "cube.mesh"),
+                                                               "rb") as b:
+        assert a.read() == b.read(), "the affine microsphere cube mesh differs"
+    asim = json.load(open(os.path.join(ax, "cube.json")))
+    out["affine_microsphere_cube_example"] = {
+        "source": "examples/solid_mechanics/hyperelastic/affine_microsphere/cube/cube.json:1-80",
+        "mesh": "neohooke_cube.npz", "simulation": asim, "max_displacement": 0.5}
     with open(os.path.join(HERE, "kats.json"), "w") as fh:
         json.dump(out, fh, indent=1, sort_keys=True)
     print("wrote", os.path.join(HERE, "kats.json"))

@@ -64,6 +64,34 @@ def test_material_factory_semantics():
         P.make_material({"shear_modulus": 1.0, "bulk_modulus": 1.0}, {"name": "unknown"})
 
 
+def test_microsphere_factory_errors():
+    """test/hyperelastic_constitutive.cpp "microsphere model error test" and the statistics
+    checks of constitutive_model_factory.cpp:48-120."""
+    ms = {"name": "microsphere"}
+    for constitutive in ({**ms, "Tyasdpe": "affine"}, {**ms, "type": "Afwsfine"},
+                         {**ms, "type": "affine", "statistics": "gaussian"},
+                         {**ms, "type": "Afwsfine", "quadrature": "BO21"},
+                         {**ms, "type": "affine", "quadrature": "BO99"},
+                         {**ms, "type": "affine", "quadrature": "BO21"},
+                         {**ms, "type": "affine", "quadrature": "BO21", "statistics": "debye"}):
+        with pytest.raises(ValueError):
+            P.make_material({}, constitutive)
+    rubber = {"elastic_modulus": 10e6, "poissons_ratio": 0.45, "segments_per_chain": 50}
+    with pytest.raises(ValueError):  # segments_per_chain missing
+        P.make_material({"elastic_modulus": 10e6, "poissons_ratio": 0.45},
+                        {**ms, "type": "affine", "quadrature": "BO21", "statistics": "langevin"})
+    for statistics, model in (("gaussian", P.GAUSS_AFFINE_MICROSPHERE),
+                              ("langevin", P.LANGEVIN_AFFINE_MICROSPHERE)):
+        m = P.make_material(rubber, {**ms, "type": "affine", "quadrature": "BO21",
+                                     "statistics": statistics})
+        assert m.model == model and m.segments_per_chain == 50
+    with pytest.raises(NotImplementedError):  # other quadrature rules and the nonaffine model
+        P.make_material(rubber, {**ms, "type": "affine", "quadrature": "FM900",
+                                 "statistics": "langevin"})
+    with pytest.raises(NotImplementedError):
+        P.make_material(rubber, {**ms, "type": "nonaffine", "quadrature": "BO21"})
+
+
 def test_dirichlet_order_and_sinusoid():
     from neon_b200 import mesh as M
     m = M.structured_hex8(2)

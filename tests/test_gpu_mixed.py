@@ -8,7 +8,7 @@ import scipy.sparse as sp
 from conftest import random_displacement, rel_err
 from neon_b200 import mesh as M
 from neon_b200 import problem as P
-from test_gpu_parity import MATERIALS, SCALE
+from test_gpu_parity import FIELD_MODELS, MATERIALS, SCALE
 
 pytestmark = pytest.mark.gpu
 
@@ -26,7 +26,7 @@ def test_matrix_free_tangent_equals_assembled(api, topo, model):
     m = M.structured_hex8(4, 3, 3, jitter=0.1, seed=3) if topo == "hex8" else \
         M.structured_tet4(3, 2, 2)
     Ge = None
-    if model == "microsphere":
+    if model in FIELD_MODELS:
         Ge = np.random.Generator(np.random.PCG64(5)).lognormal(0.0, 0.3, m.num_elements)
     g = api.SolidMesh(m.X, m.conn, MATERIALS[model], Ge)
     g.update_internal_variables(random_displacement(m, SCALE[model], 11))
@@ -38,8 +38,11 @@ def test_matrix_free_tangent_equals_assembled(api, topo, model):
 
 
 @pytest.mark.parametrize("make", [lambda: P.config_c1(6), lambda: P.config_c2(5, increments=3),
-                                  lambda: P.config_c4(4), lambda: P.config_c5_instance(3, 1.3)],
-                         ids=["c1_le_hex8", "c2_nh_hex8", "c4_microsphere_hex8", "c5_nh_tet4"])
+                                  lambda: P.config_c4(4), lambda: P.config_c5_instance(3, 1.3),
+                                  lambda: P.config_c4(4, traction=0.2, statistics="langevin",
+                                                      segments_per_chain=5)],
+                         ids=["c1_le_hex8", "c2_nh_hex8", "c4_microsphere_hex8", "c5_nh_tet4",
+                              "c4_langevin_hex8"])
 def test_mixed_newton_reaches_fp64_solution(api, make):
     pr = make()
     pr.options.residual_tolerance = pr.options.displacement_tolerance = 1e-10

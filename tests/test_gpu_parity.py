@@ -37,9 +37,17 @@ MATERIALS = {
                                     "segments_per_chain": 50},
                                    {"name": "microsphere", "type": "affine",
                                     "statistics": "gaussian", "quadrature": "BO21"}),
+    # short chains (5 segments) so the Langevin terms are far from the Gaussian limit
+    "langevin": P.make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0,
+                                 "segments_per_chain": 5},
+                                {"name": "microsphere", "type": "affine",
+                                 "statistics": "langevin", "quadrature": "BO21"}),
 }
 # displacement amplitudes that keep det F > 0 and put J2 points in the plastic range
-SCALE = {"linear_elastic": 1e-3, "neohooke": 0.02, "j2": 4e-3, "microsphere": 0.02}
+SCALE = {"linear_elastic": 1e-3, "neohooke": 0.02, "j2": 4e-3, "microsphere": 0.02,
+         "langevin": 0.03}
+# models with a per-element shear modulus field in the tests
+FIELD_MODELS = ("microsphere", "langevin")
 
 
 def _meshes():
@@ -73,7 +81,7 @@ def test_update_and_assembly_parity(api, oracle, topo, model):
     m = _meshes()[topo]
     mat = MATERIALS[model]
     Ge = None
-    if model == "microsphere":
+    if model in FIELD_MODELS:
         Ge = np.random.Generator(np.random.PCG64(5)).lognormal(0.0, 0.3, m.num_elements)
     g = api.SolidMesh(m.X, m.conn, mat, Ge)
     om = oracle.OracleMesh(m.X, m.conn, mat, Ge)
@@ -182,6 +190,10 @@ def _solve_both(api, oracle, pr, **kw):
     ("c2_neohooke_jitter", lambda: P.config_c2(5, increments=3)),
     ("c3_j2_cyclic", lambda: P.config_c3(4, steps=20)),
     ("c4_microsphere_traction", lambda: P.config_c4(4)),
+    ("c4_langevin_traction", lambda: P.config_c4(4, traction=0.2, statistics="langevin",
+                                                 segments_per_chain=5)),
+    ("affine_microsphere_cube_example",
+     lambda: cube_example_problem("affine_microsphere_cube_example")),
     ("c5_neohooke_tet4", lambda: P.config_c5_instance(3, 1.3, increments=2)),
     ("neohooke_cube_example", cube_example_problem),
 ])

@@ -115,6 +115,77 @@ def test_microsphere_known_answers(oracle, kats):
     assert all(np.linalg.norm(s) > 0 for s in om.get("sigma"))
 
 
+def _langevin(E, nu, N):
+    return P.make_material({"elastic_modulus": E, "poissons_ratio": nu, "segments_per_chain": N},
+                           {"name": "microsphere", "type": "affine", "statistics": "langevin",
+                            "quadrature": "BO21"})
+
+
+def _uniaxial(om, lam):
+    F = np.diag([lam, 1 / np.sqrt(lam), 1 / np.sqrt(lam)]).reshape(-1)
+    om.set("F", np.tile(F, (2, 1)))
+    om.set("detF", np.full(2, np.linalg.det(F.reshape(3, 3))))
+    om.constitutive_only()
+
+
+def test_langevin_microsphere_known_answers(oracle, kats):
+    """test/hyperelastic_constitutive.cpp "Affine microsphere": no stress and a symmetric positive
+    definite tangent at F = I, a symmetric positive definite tangent under uniaxial stretch."""
+    k = kats["langevin_affine_microsphere"]
+    mat = _langevin(k["E"], k["nu"], k["segments_per_chain"])
+    assert mat.model == P.LANGEVIN_AFFINE_MICROSPHERE
+    om = _single_point(oracle, mat)
+    om.set("F", np.tile(np.eye(3).reshape(-1), (2, 1)))
+    om.set("detF", np.ones(2))
+    om.constitutive_only()
+    assert all(_is_spd(D) for D in om.get("D"))
+    assert np.abs(om.get("sigma")).max() / mat.G < 1e-5
+    _uniaxial(om, k["uniaxial_stretch"])
+    assert all(_is_spd(D) for D in om.get("D"))
+    assert all(np.linalg.norm(s) > 0 for s in om.get("sigma"))
+
+
+def test_langevin_tends_to_gaussian_for_long_chains(oracle):
+    """pade_first -> 3 and pade_second - pade_first -> 0 as N -> infinity: the Langevin model
+    becomes the Gaussian one (tau = 3 G sum w t(x)t, zero macro moduli)."""
+    gauss = P.make_material({"elastic_modulus": 10e6, "poissons_ratio": 0.45,
+                             "segments_per_chain": 50},
+                            {"name": "microsphere", "type": "affine", "statistics": "gaussian",
+                             "quadrature": "BO21"})
+    og, ol = _single_point(oracle, gauss), _single_point(oracle, _langevin(10e6, 0.45, 1e12))
+    for om in (og, ol):
+        _uniaxial(om, 1.3)
+    assert np.abs(ol.get("sigma") - og.get("sigma")).max() < 1e-9 * np.abs(og.get("sigma")).max()
+    assert np.abs(ol.get("D") - og.get("D")).max() < 1e-9 * np.abs(og.get("D")).max()
+
+
+def test_langevin_chains_stiffen_with_stretch(oracle):
+    """Finite chains lock: the ratio of the Langevin to the Gaussian uniaxial stress grows with
+    the stretch and with fewer segments per chain."""
+    gauss = P.make_material({"elastic_modulus": 1.0, "poissons_ratio": 0.45,
+                             "segments_per_chain": 50},
+                            {"name": "microsphere", "type": "affine", "statistics": "gaussian",
+                             "quadrature": "BO21"})
+    ratios = {}
+    for N in (5.0, 20.0):
+        for lam in (1.2, 1.6):
+            og, ol = _single_point(oracle, gauss), _single_point(oracle, _langevin(1.0, 0.45, N))
+            _uniaxial(og, lam)
+            _uniaxial(ol, lam)
+            ratios[N, lam] = ol.get("sigma")[0][0] / og.get("sigma")[0][0]
+    assert ratios[5.0, 1.6] > ratios[5.0, 1.2] > 1.0
+    assert ratios[5.0, 1.6] > ratios[20.0, 1.6] > 1.0
+
+
+def test_langevin_cube_example_deck(kats):
+    """The affine microsphere cube example's deck builds the Langevin model on the shared cube
+    mesh (examples/.../affine_microsphere/cube/cube.json)."""
+    pr = cube_example_problem("affine_microsphere_cube_example")
+    assert pr.material.model == P.LANGEVIN_AFFINE_MICROSPHERE
+    assert pr.material.segments_per_chain == 45
+    assert pr.mesh.conn.shape[1] == 8
+
+
 def test_cg_three_by_three(oracle, kats):
     k = kats["cg_3x3"]
     import scipy.sparse as sp
