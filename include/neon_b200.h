@@ -7,7 +7,8 @@
  *     (src/mesh/mechanics/solid/submesh.cpp:66-269, mesh.cpp:56-76),
  *   the constitutive plugins on the path
  *     (src/constitutive/mechanics/solid/{isotropic_linear_elasticity,compressible_neohooke,
- *      small_strain_J2_plasticity,gaussian_affine_microsphere,affine_microsphere}.cpp),
+ *      small_strain_J2_plasticity,gaussian_affine_microsphere,affine_microsphere,
+ *      nonaffine_microsphere}.cpp),
  *   and the linear_solver plugin (src/solver/linear/linear_solver.hpp:13-71).
  *
  * Plain C types only.  Every call returns an nb2_status; nothing throws across the boundary.
@@ -47,8 +48,10 @@ typedef enum nb2_model {
     NB2_NEOHOOKE = 1,                    /* "neohooke" */
     NB2_SMALL_STRAIN_J2_PLASTICITY = 2,  /* "J2_plasticity", "finite_strain": false */
     NB2_GAUSSIAN_AFFINE_MICROSPHERE = 3, /* "microsphere", "affine", "gaussian", "BO21" */
-    NB2_LANGEVIN_AFFINE_MICROSPHERE = 4  /* "microsphere", "affine", "langevin", "BO21"
+    NB2_LANGEVIN_AFFINE_MICROSPHERE = 4, /* "microsphere", "affine", "langevin", "BO21"
                                             (affine_microsphere.cpp:23-112) */
+    NB2_NONAFFINE_MICROSPHERE = 5        /* "microsphere", "nonaffine", "BO21"
+                                            (nonaffine_microsphere.cpp:29-175) */
 } nb2_model;
 
 /* Precision of the stiffness / inner linear solve. */
@@ -75,8 +78,9 @@ typedef struct nb2_mesh_desc {
 /* Material parameters as neon stores them: bulk modulus K and shear modulus G
  * (isotropic_elastic_property.cpp:10-43, lambda = K - 2G/3), yield stress and linear isotropic
  * hardening (isotropic_elastic_plastic.cpp:31-38), segments per chain
- * (micromechanical_elastomer.cpp:13-21; used by Langevin statistics, required but unused by
- * Gaussian statistics). */
+ * (micromechanical_elastomer.cpp:13-21; used by Langevin statistics and the non-affine model,
+ * required but unused by Gaussian statistics), the non-affine stretch parameter p
+ * (nonaffine_microsphere.cpp:17-25; non-affine model only). */
 typedef struct nb2_material {
     int32_t model; /* nb2_model */
     double bulk_modulus;
@@ -84,6 +88,7 @@ typedef struct nb2_material {
     double yield_stress;
     double isotropic_hardening_modulus;
     double segments_per_chain;
+    double nonaffine_stretch_parameter;
 } nb2_material;
 
 /* A time/value table applied to a DOF list: a Dirichlet boundary (mesh/boundary/nodal_value.cpp,

@@ -52,7 +52,8 @@ class MaterialDesc(C.Structure):
     _fields_ = [("model", C.c_int32), ("bulk_modulus", C.c_double),
                 ("shear_modulus", C.c_double), ("yield_stress", C.c_double),
                 ("isotropic_hardening_modulus", C.c_double),
-                ("segments_per_chain", C.c_double)]
+                ("segments_per_chain", C.c_double),
+                ("nonaffine_stretch_parameter", C.c_double)]
 
 
 class DofTableDesc(C.Structure):
@@ -174,7 +175,8 @@ class SolidMesh:
         desc = MeshDesc(self.X.shape[0], self.X.ctypes.data, self.conn.shape[0],
                         self.conn.shape[1], self.conn.ctypes.data)
         mat = MaterialDesc(int(material.model), material.K, material.G, material.yield_stress,
-                           material.hardening, material.segments_per_chain)
+                           material.hardening, material.segments_per_chain,
+                           material.nonaffine_stretch_parameter)
         h = P()
         _check(L.nb2_create(C.byref(desc), C.byref(mat), C.byref(h)), None, "nb2_create")
         self.h = h

@@ -9,18 +9,18 @@
 //            precision, in two passes of at most 3 blocks (fewer live registers), and adds
 //            them (and their mirrored blocks) to K with red.global.add.
 // Shared memory per element holds L (Real) for every point, the flow direction N (J2) or the
-// anisotropic tangent s Da (Langevin microsphere) and, for finite-strain models, g = s sigma L
+// anisotropic tangent s Da (Langevin and non-affine microsphere) and, for finite-strain models, g = s sigma L
 // (FP64) used by the geometric stiffness.
 #pragma once
 
 template <int NPE, int MODEL, typename Real, int MODE>
-__global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : ((MODEL == MODEL_ML) ? 4 : 8))
+__global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : (model_aniso(MODEL) ? 4 : 8))
     k_element(ElementArgs A) {
     using T = Topo<NPE>;
     constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC, MAXB = T::MAXB;
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || MODEL == MODEL_ML);
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || model_aniso(MODEL));
     constexpr bool kJ2 = (MODEL == MODEL_J2);
-    constexpr bool kAniso = (MODEL == MODEL_ML);
+    constexpr bool kAniso = model_aniso(MODEL);
     constexpr bool kCon = (MODE & MODE_CONSTITUTIVE) != 0;
     constexpr bool kStiff = (MODE & MODE_STIFFNESS) != 0;
     constexpr bool kForce = (MODE & MODE_FORCE) != 0;
@@ -126,8 +126,10 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : ((MODEL == MODEL
                     if (!cm_j2(A, q, Hm, o)) report_status(A, e, NB2_E_RETURN_MAP);
                 } else if constexpr (MODEL == MODEL_MS) {
                     cm_microsphere(Ae, Ae.G, Fd, detF, o);
-                } else {
+                } else if constexpr (MODEL == MODEL_ML) {
                     cm_langevin(Ae, Ae.G, Fd, detF, o);
+                } else {
+                    cm_nonaffine(Ae, Ae.G, Fd, detF, o);
                 }
                 bool bad = isnan(o.lam) || isnan(o.mu);
 #pragma unroll

@@ -315,6 +315,131 @@ __device__ __forceinline__ void cm_langevin(const ElementArgs& A, double Gm, con
     o.b = 0.0;
 }
 
+// P C P for a packed symmetric 6x6 C in kinetic Voigt, P the deviatoric projector (normal block
+// I - 1/3 1 1^T, shear block I): subtract the normal-row means on both sides
+__device__ __forceinline__ void project_deviatoric(const double* C, double* Da) {
+    double cm[6];
+#pragma unroll
+    for (int w = 0; w < 6; ++w) cm[w] = (C[sym6(0, w)] + C[sym6(1, w)] + C[sym6(2, w)]) / 3.0;
+    const double mm = (cm[0] + cm[1] + cm[2]) / 3.0;
+#pragma unroll
+    for (int v = 0; v < 6; ++v)
+#pragma unroll
+        for (int w = v; w < 6; ++w) {
+            double d = C[sym6(v, w)];
+            if (v < 3 && w < 3)
+                d += mm - cm[v] - cm[w];
+            else if (v < 3)
+                d -= cm[w];
+            Da[sym6(v, w)] = d;
+        }
+}
+
+// nonaffine_microsphere.cpp:29-175 (tube geometry U = 9 and tube parameter q = 1 are members of
+// the reference class; the stretch parameter p comes from the material).  One pass over the 21
+// directions accumulates, with t = Fbar r, l = |t|, n = Fbar^-T r, nu = |n|:
+//   sum w l^p,  h = sum w l^(p-2) t(x)t,  H/(p-2) = sum w l^(p-4) t(x)t(x)t(x)t,
+//   k = sum w nu^-1 n(x)n,  K + G = sum w (-nu^-3 n(x)n(x)n(x)n + 2 nu^-1 o(n))   (q = 1);
+// then lambda = (sum w l^p)^(1/p) and, with pf, ps the Pade approximants at lambda,
+//   tau = G pf lambda^(2-p) h - G N U k,
+//   C   = (G ps - (p-1) G pf) lambda^(2-2p) h(x)h + G pf lambda^(2-p) H + G N U (K + G);
+// the tangent is the affine model's: lam', mu' from tau and Da = P C P.
+__device__ __forceinline__ void cm_nonaffine(const ElementArgs& A, double Gm, const double* F,
+                                             double J, QpOut& o) {
+    constexpr double U = 9.0;
+    const double K = A.K, Nc = A.Nseg, pp = A.p_na;
+    const double sc = pow(det3(F), -1.0 / 3.0);
+    double Fb[9], Fbi[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Fb[i] = sc * F[i];
+    inv3(Fb, Fbi);
+    double lp = 0.0, h[6] = {0, 0, 0, 0, 0, 0}, k[6] = {0, 0, 0, 0, 0, 0};
+    double H[21], C[21];
+#pragma unroll
+    for (int c = 0; c < 21; ++c) H[c] = C[c] = 0.0;
+#pragma unroll 1
+    for (int i = 0; i < 21; ++i) {
+        const double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1], r2 = c_sphere_r[3 * i + 2];
+        const double w = c_sphere_w[i];
+        const double t[3] = {Fb[0] * r0 + Fb[1] * r1 + Fb[2] * r2,
+                             Fb[3] * r0 + Fb[4] * r1 + Fb[5] * r2,
+                             Fb[6] * r0 + Fb[7] * r1 + Fb[8] * r2};
+        const double n[3] = {Fbi[0] * r0 + Fbi[3] * r1 + Fbi[6] * r2,
+                             Fbi[1] * r0 + Fbi[4] * r1 + Fbi[7] * r2,
+                             Fbi[2] * r0 + Fbi[5] * r1 + Fbi[8] * r2};
+        const double l2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+        const double nu = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        const double lpw = pow(sqrt(l2), pp);
+        lp += lpw * w;
+        const double a2 = w * lpw / l2, a4 = a2 / l2;      // w l^(p-2), w l^(p-4)
+        const double b1 = w / nu, b3 = b1 / (nu * nu);      // w nu^-1, w nu^-3
+        const double tv[6] = {t[0] * t[0], t[1] * t[1], t[2] * t[2], t[1] * t[2], t[0] * t[2],
+                              t[0] * t[1]};
+        const double nv[6] = {n[0] * n[0], n[1] * n[1], n[2] * n[2], n[1] * n[2], n[0] * n[2],
+                              n[0] * n[1]};
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            h[c] += a2 * tv[c];
+            k[c] += b1 * nv[c];
+        }
+#pragma unroll
+        for (int v = 0; v < 6; ++v)
+#pragma unroll
+            for (int u = v; u < 6; ++u) {
+                H[sym6(v, u)] += a4 * tv[v] * tv[u];
+                C[sym6(v, u)] -= b3 * nv[v] * nv[u];
+            }
+        // 2 o(n) (compute_o_dot_product), upper triangle
+        const double b2 = 2.0 * b1;
+        C[sym6(0, 0)] += b2 * 2.0 * nv[0];
+        C[sym6(1, 1)] += b2 * 2.0 * nv[1];
+        C[sym6(2, 2)] += b2 * 2.0 * nv[2];
+        C[sym6(0, 4)] += b2 * nv[4];
+        C[sym6(0, 5)] += b2 * nv[5];
+        C[sym6(1, 3)] += b2 * nv[3];
+        C[sym6(1, 5)] += b2 * nv[5];
+        C[sym6(2, 3)] += b2 * nv[3];
+        C[sym6(2, 4)] += b2 * nv[4];
+        C[sym6(3, 3)] += b2 * 0.5 * (nv[1] + nv[2]);
+        C[sym6(3, 4)] += b2 * 0.5 * nv[5];
+        C[sym6(3, 5)] += b2 * 0.5 * nv[4];
+        C[sym6(4, 4)] += b2 * 0.5 * (nv[0] + nv[2]);
+        C[sym6(4, 5)] += b2 * 0.5 * nv[3];
+        C[sym6(5, 5)] += b2 * 0.5 * (nv[0] + nv[1]);
+    }
+    const double lam = pow(lp, 1.0 / pp);
+    const double d = Nc - lam * lam;
+    const double pf = (3.0 * Nc - lam * lam) / d;
+    const double ps = (lam * lam * lam * lam + 3.0 * Nc * Nc) / (d * d);
+    const double micro_tau = Gm * pf * lam;
+    const double cf = micro_tau * pow(lam, 1.0 - pp);
+    const double chh = Gm * ps * pow(lam, 2.0 - 2.0 * pp) -
+                       (pp - 1.0) * micro_tau * pow(lam, 1.0 - 2.0 * pp);
+    const double gnu = Gm * Nc * U;
+    double tau[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tau[c] = cf * h[c] - gnu * k[c];
+#pragma unroll
+    for (int v = 0; v < 6; ++v)
+#pragma unroll
+        for (int u = v; u < 6; ++u)
+            C[sym6(v, u)] = chh * h[v] * h[u] + cf * (pp - 2.0) * H[sym6(v, u)] + gnu * C[sym6(v, u)];
+    project_deviatoric(C, o.Da);
+    const double p = J * (K / 2.0 * (J - 1.0 / J));
+    const double trt = tau[0] + tau[1] + tau[2];
+    const double tr3 = trt / 3.0;
+    o.sig[0] = (p + tau[0] - tr3) / J;
+    o.sig[1] = (p + tau[1] - tr3) / J;
+    o.sig[2] = (p + tau[2] - tr3) / J;
+    o.sig[3] = tau[3] / J;
+    o.sig[4] = tau[4] / J;
+    o.sig[5] = tau[5] / J;
+    const double kappa = (J * J) * (K / 2.0 * (1.0 + 1.0 / (J * J)));
+    o.lam = kappa + p - (2.0 / 9.0) * trt;
+    o.mu = trt / 3.0 - p;
+    o.b = 0.0;
+}
+
 // y += B_a^T Da B_b restricted to one 3x3 block: K[i][k] += sum_vw B_a[v][i] Da[v][w] B_b[w][k]
 // with the kinematic strain operator B (rows 11 22 33 23 13 12; shear rows engineering).
 // Column k of B_b has three entries: k=0 -> rows (0, 4, 5) = (L0, L2, L1), k=1 -> (1, 3, 5) =
@@ -390,9 +515,9 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
                                               double* __restrict__ y) {
     using T = Topo<NPE>;
     constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC;
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || MODEL == MODEL_ML);
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || model_aniso(MODEL));
     constexpr bool kJ2 = (MODEL == MODEL_J2);
-    constexpr bool kAniso = (MODEL == MODEL_ML);
+    constexpr bool kAniso = model_aniso(MODEL);
     __shared__ double sx[EPC][NPE][3];
     __shared__ double sv[EPC][NPE][3];
     __shared__ double sdN[NQ][NPE][3];
@@ -928,6 +1053,7 @@ static int dispatch_model(nb2_ctx* c, const ElementArgs& A, int mode, int precis
         case MODEL_J2: return dispatch_mode<NPE, MODEL_J2>(c, A, mode, precision);
         case MODEL_MS: return dispatch_mode<NPE, MODEL_MS>(c, A, mode, precision);
         case MODEL_ML: return dispatch_mode<NPE, MODEL_ML>(c, A, mode, precision);
+        case MODEL_MN: return dispatch_mode<NPE, MODEL_MN>(c, A, mode, precision);
     }
     return NB2_E_INPUT;
 }
@@ -943,6 +1069,7 @@ static void launch_apply_t(nb2_ctx* c, const ElementArgs& A, const double* v, do
         case MODEL_NH: k_apply<NPE, MODEL_NH><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         case MODEL_J2: k_apply<NPE, MODEL_J2><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         case MODEL_ML: k_apply<NPE, MODEL_ML><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+        case MODEL_MN: k_apply<NPE, MODEL_MN><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         default: k_apply<NPE, MODEL_MS><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
     }
     c->launches++;
@@ -986,6 +1113,7 @@ int launch_mf_setup(nb2_ctx* c) {
         case MODEL_NH: hex ? mf_setup_t<8, MODEL_NH>(c, A) : mf_setup_t<4, MODEL_NH>(c, A); break;
         case MODEL_J2: hex ? mf_setup_t<8, MODEL_J2>(c, A) : mf_setup_t<4, MODEL_J2>(c, A); break;
         case MODEL_ML: hex ? mf_setup_t<8, MODEL_ML>(c, A) : mf_setup_t<4, MODEL_ML>(c, A); break;
+        case MODEL_MN: hex ? mf_setup_t<8, MODEL_MN>(c, A) : mf_setup_t<4, MODEL_MN>(c, A); break;
         default: hex ? mf_setup_t<8, MODEL_MS>(c, A) : mf_setup_t<4, MODEL_MS>(c, A); break;
     }
     NB2_CUDA(c, cudaGetLastError());
@@ -998,6 +1126,7 @@ int mf_coefficients(int model) {
         case MODEL_NH: return MfCoef<MODEL_NH>::KC;
         case MODEL_J2: return MfCoef<MODEL_J2>::KC;
         case MODEL_ML: return MfCoef<MODEL_ML>::KC;
+        case MODEL_MN: return MfCoef<MODEL_MN>::KC;
         default: return MfCoef<MODEL_MS>::KC;
     }
 }
@@ -1017,6 +1146,7 @@ void enqueue_apply32(nb2_ctx* c, const float* v, float* ye, const int* done) {
         case MODEL_NH: hex ? apply32_t<8, MODEL_NH>(c, v, ye, done) : apply32_t<4, MODEL_NH>(c, v, ye, done); break;
         case MODEL_J2: hex ? apply32_t<8, MODEL_J2>(c, v, ye, done) : apply32_t<4, MODEL_J2>(c, v, ye, done); break;
         case MODEL_ML: hex ? apply32_t<8, MODEL_ML>(c, v, ye, done) : apply32_t<4, MODEL_ML>(c, v, ye, done); break;
+        case MODEL_MN: hex ? apply32_t<8, MODEL_MN>(c, v, ye, done) : apply32_t<4, MODEL_MN>(c, v, ye, done); break;
         default: hex ? apply32_t<8, MODEL_MS>(c, v, ye, done) : apply32_t<4, MODEL_MS>(c, v, ye, done); break;
     }
 }
@@ -1077,6 +1207,7 @@ static ElementArgs make_args(nb2_ctx* c) {
     A.sigma_y = c->mat.yield_stress;
     A.H_iso = c->mat.isotropic_hardening_modulus;
     A.Nseg = c->mat.segments_per_chain;
+    A.p_na = c->mat.nonaffine_stretch_parameter;
     A.Ge = c->Ge;
     A.Ke = c->Ke;
     A.ep = c->ep;
@@ -1119,17 +1250,19 @@ int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
 
 // Canonical algorithmic FLOPs per element (hex8 small strain 29,040; hex8 finite strain 32,240;
 // tet4 finite strain 1,552) plus the constitutive update per point (LE 60, NH 120, J2 250,
-// microsphere BO21 2,000, Langevin microsphere BO21 3,000); the Langevin anisotropic tangent
+// microsphere BO21 2,000, Langevin microsphere BO21 3,000, non-affine BO21 4,500); the
+// anisotropic tangent of the Langevin and non-affine models
 // adds 81 FMAs per block and point (hex8 36 blocks x 8 points, tet4 10 x 1).
 void element_flop_model(const nb2_ctx* c, double* flops_per_element) {
     double base;
-    bool finite = c->mat.model == MODEL_NH || c->mat.model == MODEL_MS || c->mat.model == MODEL_ML;
+    bool finite = c->mat.model == MODEL_NH || c->mat.model == MODEL_MS ||
+                  model_aniso(c->mat.model);
     if (c->npe == 8)
         base = finite ? 32240.0 : 29040.0;
     else
         base = 1552.0;
-    if (c->mat.model == MODEL_ML) base += 2.0 * 81.0 * (c->npe == 8 ? 36 * 8 : 10);
-    const double cm[5] = {60.0, 120.0, 250.0, 2000.0, 3000.0};
+    if (model_aniso(c->mat.model)) base += 2.0 * 81.0 * (c->npe == 8 ? 36 * 8 : 10);
+    const double cm[6] = {60.0, 120.0, 250.0, 2000.0, 3000.0, 4500.0};
     *flops_per_element = base + c->nq * cm[c->mat.model];
 }
 

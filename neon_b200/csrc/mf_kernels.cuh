@@ -5,7 +5,7 @@
 // The same operator applied element by element needs far less: per element the FP32 node
 // coordinates relative to its first node (96 B; differences taken in FP64, so no cancellation
 // in FP32), per quadrature point the tangent coefficients pre-multiplied by w det J (2 floats;
-// J2 plastic points 9, finite strain 8, Langevin microsphere 8 + 21), the node indices, and the
+// J2 plastic points 9, finite strain 8, anisotropic microspheres 8 + 21), the node indices, the
 // input/output vectors.
 //   k_mf_setup  once per linear solve (after an element pass that stored its outputs): writes
 //               those FP32 data and each element's contribution to diag(K) (Jacobi);
@@ -41,22 +41,22 @@ __device__ __forceinline__ void inv3f(const float* m, float* r) {
 template <int MODEL>
 struct MfCoef {
     static constexpr int KC =
-        (MODEL == MODEL_J2) ? 9 : ((MODEL == MODEL_LE) ? 2 : ((MODEL == MODEL_ML) ? 8 + 21 : 8));
+        (MODEL == MODEL_J2) ? 9 : ((MODEL == MODEL_LE) ? 2 : (model_aniso(MODEL) ? 8 + 21 : 8));
 };
 
 // Setup from the stored FP64 outputs of the last MODE_STORE pass (A.u = its displacement):
 //   md[e][3a+k]  = (float)(x_a - x_0)_k
 //   mc[c][q]     = s lam', s mu' | J2: s b, N (6) | finite strain: s sigma (6)
-//                  | Langevin microsphere: then s Da (21, packed upper triangle)
+//                  | Langevin / non-affine microsphere: then s Da (21, packed upper triangle)
 //   de[e][3a+i]  = element contribution to K_(3a+i, 3a+i)
 template <int NPE, int MODEL>
 __global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restrict__ md,
                                                  float* __restrict__ mc, float* __restrict__ de) {
     using T = Topo<NPE>;
     constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC;
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || MODEL == MODEL_ML);
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || model_aniso(MODEL));
     constexpr bool kJ2 = (MODEL == MODEL_J2);
-    constexpr bool kAniso = (MODEL == MODEL_ML);
+    constexpr bool kAniso = model_aniso(MODEL);
     __shared__ double sx[EPC][NPE][3];
     __shared__ double sdN[NQ][NPE][3];
     __shared__ double sD[EPC][NQ][NPE * 3];
@@ -196,7 +196,7 @@ template <int MODEL>
 __device__ __forceinline__ void point_flux(const float* J, const float* Gx,
                                            const float* __restrict__ mc, long long nqp,
                                            long long q, float* Pm) {
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || MODEL == MODEL_ML);
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || model_aniso(MODEL));
     constexpr bool kJ2 = (MODEL == MODEL_J2);
     float Ji[9];
     inv3f(J, Ji);
@@ -231,7 +231,7 @@ __device__ __forceinline__ void point_flux(const float* J, const float* Gx,
             S[1] += bN * N6[5]; S[3] += bN * N6[5];
         }
     }
-    if constexpr (MODEL == MODEL_ML) {
+    if constexpr (model_aniso(MODEL)) {
         float Da[21], sa[6];
 #pragma unroll
         for (int c = 0; c < 21; ++c) Da[c] = mc[(8 + c) * nqp + q];

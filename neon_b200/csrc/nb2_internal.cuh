@@ -22,14 +22,21 @@ namespace nb2 {
 //   qp state     SoA: ep[6][nqp], epbar[nqp] (current) and their committed copies
 //   qp outputs   sig[6][nqp], dpar[rows][nqp], detF[nqp] (only for the split update/assemble
 //                path); dpar rows: lam', mu', b, then the J2 flow direction N (6) or, for the
-//                Langevin microsphere, the anisotropic tangent (21, packed upper triangle)
+//                Langevin and non-affine microsphere, the anisotropic tangent (21, packed
+//                upper triangle)
 // ---------------------------------------------------------------------------------------
 
-// MODEL_MS: Gaussian affine microsphere, MODEL_ML: Langevin affine microsphere
-enum : int { MODEL_LE = 0, MODEL_NH = 1, MODEL_J2 = 2, MODEL_MS = 3, MODEL_ML = 4 };
+// MODEL_MS: Gaussian affine microsphere, MODEL_ML: Langevin affine microsphere,
+// MODEL_MN: non-affine microsphere
+enum : int { MODEL_LE = 0, MODEL_NH = 1, MODEL_J2 = 2, MODEL_MS = 3, MODEL_ML = 4, MODEL_MN = 5 };
+
+// models whose tangent carries a general anisotropic part Da (packed 6x6) besides lam', mu'
+__host__ __device__ constexpr bool model_aniso(int model) {
+    return model == MODEL_ML || model == MODEL_MN;
+}
 
 // rows of dpar for a model
-inline int dpar_rows(int model) { return model == MODEL_ML ? 3 + 21 : 9; }
+inline int dpar_rows(int model) { return model_aniso(model) ? 3 + 21 : 9; }
 
 // Packed index of the symmetric 6x6 (kinetic Voigt 11 22 33 23 13 12) entry (v, w): the upper
 // triangle row by row.
@@ -59,7 +66,8 @@ struct ElementArgs {
     int E;
     int nqp;
     double K, G, lambda, sigma_y, H_iso;
-    double Nseg;       // segments per chain (Langevin microsphere)
+    double Nseg;       // segments per chain (Langevin and non-affine microsphere)
+    double p_na;       // non-affine stretch parameter
     const double* Ge;  // per-element shear modulus (or null)
     const double* Ke;  // per-element bulk modulus (or null)
     double* ep;      // [6][nqp]

@@ -15,7 +15,7 @@ from .mesh import Mesh, quad4_consistent_forces, structured_hex8, structured_tet
 
 # Model identifiers of the C-ABI (include/neon_b200.h, enum nb2_model)
 LINEAR_ELASTIC, NEO_HOOKE, J2_SMALL_STRAIN, GAUSS_AFFINE_MICROSPHERE = 0, 1, 2, 3
-LANGEVIN_AFFINE_MICROSPHERE = 4
+LANGEVIN_AFFINE_MICROSPHERE, NONAFFINE_MICROSPHERE = 4, 5
 
 MODEL_NAMES = {
     LINEAR_ELASTIC: "isotropic_linear_elasticity",
@@ -23,6 +23,7 @@ MODEL_NAMES = {
     J2_SMALL_STRAIN: "J2_plasticity",
     GAUSS_AFFINE_MICROSPHERE: "microsphere",
     LANGEVIN_AFFINE_MICROSPHERE: "microsphere",
+    NONAFFINE_MICROSPHERE: "microsphere",
 }
 
 
@@ -31,13 +32,15 @@ class Material:
     """Isotropic parameters as neon stores them: bulk and shear modulus
     (material/isotropic_elastic_property.cpp:10-43), yield stress and linear isotropic hardening
     (material/isotropic_elastic_plastic.cpp:10-38), segments per chain
-    (material/micromechanical_elastomer.cpp:13-21)."""
+    (material/micromechanical_elastomer.cpp:13-21), the non-affine stretch parameter
+    (constitutive/mechanics/solid/nonaffine_microsphere.cpp:17-25)."""
     model: int
     K: float
     G: float
     yield_stress: float = 0.0
     hardening: float = 0.0
     segments_per_chain: float = 0.0
+    nonaffine_stretch_parameter: float = 0.0
 
     @property
     def lam(self) -> float:
@@ -45,7 +48,8 @@ class Material:
 
     def params(self) -> np.ndarray:
         return np.array([self.K, self.G, self.yield_stress, self.hardening,
-                         self.segments_per_chain], dtype=np.float64)
+                         self.segments_per_chain, self.nonaffine_stretch_parameter],
+                        dtype=np.float64)
 
 
 def _check_microsphere_options(constitutive: dict):
@@ -103,15 +107,23 @@ def make_material(material: dict, constitutive: dict) -> Material:
         return Material(J2_SMALL_STRAIN, K, G, float(material["yield_stress"]),
                         float(material.get("isotropic_hardening_modulus", 0.0)))
     if name == "microsphere":
-        if constitutive["type"] != "affine" or constitutive["quadrature"] != "BO21" \
-                or ("ageing" in constitutive and constitutive["statistics"] == "gaussian"):
-            raise NotImplementedError("only the affine BO21 microsphere (Gaussian or Langevin "
-                                      "statistics) is on this path")
+        affine = constitutive["type"] == "affine"
+        if constitutive["quadrature"] != "BO21" or \
+                (affine and "ageing" in constitutive and constitutive["statistics"] == "gaussian"):
+            raise NotImplementedError("only the BO21 microsphere models (affine Gaussian, affine "
+                                      "Langevin, non-affine) are on this path")
         if "segments_per_chain" not in material:
             raise ValueError("segments_per_chain not specified in material data")
+        N = float(material["segments_per_chain"])
+        if not affine:
+            if "nonaffine_stretch_parameter" not in material:
+                raise ValueError('"nonaffine_stretch_parameter" not specified in material data')
+            return Material(NONAFFINE_MICROSPHERE, K, G, segments_per_chain=N,
+                            nonaffine_stretch_parameter=float(
+                                material["nonaffine_stretch_parameter"]))
         model = GAUSS_AFFINE_MICROSPHERE if constitutive["statistics"] == "gaussian" \
             else LANGEVIN_AFFINE_MICROSPHERE
-        return Material(model, K, G, segments_per_chain=float(material["segments_per_chain"]))
+        return Material(model, K, G, segments_per_chain=N)
     raise ValueError(f"The model name {name} is not recognised")
 
 
@@ -253,15 +265,21 @@ def config_c3(n: int = 100, steps: int = 20, increments_per_step: int = 4) -> Pr
 
 
 def config_c4(n: int = 48, seed_field: int = 7, traction: float = 0.05,
-              statistics: str = "gaussian", segments_per_chain: float = 50.0) -> Problem:
+              statistics: str = "gaussian", segments_per_chain: float = 50.0,
+              nonaffine_stretch_parameter: float = 1.0) -> Problem:
     """Affine microsphere (BO21, K=100, G=1 scaled by a per-element lognormal(0, 0.3) field;
-    Gaussian chains, or Langevin chains of ``segments_per_chain`` segments), n^3 hex8, bottom
-    clamped, uniform top traction in z (consistent quad4 forces)."""
+    Gaussian chains, or Langevin chains of ``segments_per_chain`` segments; ``statistics=
+    "nonaffine"`` for the non-affine model), n^3 hex8, bottom clamped, uniform top traction in z
+    (consistent quad4 forces)."""
     mesh = structured_hex8(n)
+    constitutive = {"name": "microsphere", "type": "affine", "statistics": statistics,
+                    "quadrature": "BO21"}
+    if statistics == "nonaffine":
+        constitutive = {"name": "microsphere", "type": "nonaffine", "quadrature": "BO21"}
     mat = make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0,
-                         "segments_per_chain": segments_per_chain},
-                        {"name": "microsphere", "type": "affine", "statistics": statistics,
-                         "quadrature": "BO21"})
+                         "segments_per_chain": segments_per_chain,
+                         "nonaffine_stretch_parameter": nonaffine_stretch_parameter},
+                        constitutive)
     rng = np.random.Generator(np.random.PCG64(seed_field))
     Ge = rng.lognormal(mean=0.0, sigma=0.3, size=mesh.num_elements) * mat.G
     bcs = [{"name": "bottom", "time": [0.0, 1.0], "x": [0.0, 0.0], "y": [0.0, 0.0],

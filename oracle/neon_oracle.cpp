@@ -75,7 +75,8 @@ enum : int {
     NEO_HOOKE = 1,
     J2_SMALL_STRAIN = 2,
     GAUSS_AFFINE_MICROSPHERE = 3,
-    LANGEVIN_AFFINE_MICROSPHERE = 4
+    LANGEVIN_AFFINE_MICROSPHERE = 4,
+    NONAFFINE_MICROSPHERE = 5
 };
 
 // ----------------------------------------------------------------------------------------
@@ -260,6 +261,7 @@ struct Material {
     double K = 0, G = 0;             // isotropic_elastic_property.cpp:10-43
     double sigma_y = 0, H_iso = 0;   // isotropic_elastic_plastic.cpp:10-38
     double segments = 0;             // micromechanical_elastomer.cpp:13-21
+    double nonaffine_p = 0;          // nonaffine_microsphere.cpp:17-25
     double lambda() const { return K - 2.0 * G / 3.0; }  // isotropic_elastic_property.hpp:28
 };
 
@@ -432,15 +434,14 @@ double pade_second(double l, double N) {
     return (std::pow(l, 4) + 3.0 * std::pow(N, 2)) / std::pow(N - std::pow(l, 2), 2);
 }
 
+void microsphere_response(Oracle& o, size_t q, const double* tau, const double* macroC);
+
 void update_microsphere(Oracle& o, size_t q, double G, bool langevin = false) {
     const double Nseg = o.mat.segments;
-    const double K = o.mat.K;
     const double* Fq = &o.F[q * 9];
-    double J = o.detF[q];
     double scale = std::pow(det3(Fq), -1.0 / 3.0);
     double Fb[9];
     for (int i = 0; i < 9; ++i) Fb[i] = scale * Fq[i];
-    double pressure = J * (K / 2.0 * (J - 1.0 / J));
     // compute_macro_stress: 3 G sum_i w_i t_i (x) t_i, t_i = Fbar r_i (Gaussian), or
     // G sum_i w_i pade_first t_i (x) t_i (Langevin); compute_macro_moduli (Langevin)
     double acc[9] = {0};
@@ -468,6 +469,15 @@ void update_microsphere(Oracle& o, size_t q, double G, bool langevin = false) {
     double tau[9];
     for (int i = 0; i < 9; ++i) tau[i] = (langevin ? G : 3.0 * G) * acc[i];
     for (int i = 0; i < 36; ++i) macroC[i] *= G;
+    microsphere_response(o, q, tau, macroC);
+}
+
+// affine_microsphere::compute_kirchhoff_stress and compute_material_tangent
+// (affine_microsphere.cpp:55-77), shared by the affine and non-affine models
+void microsphere_response(Oracle& o, size_t q, const double* tau, const double* macroC) {
+    const double K = o.mat.K;
+    const double J = o.detF[q];
+    const double pressure = J * (K / 2.0 * (J - 1.0 / J));
     // Kirchhoff stress p I + dev(tau) -> Cauchy / J
     double dev[9];
     deviatoric3(tau, dev);
@@ -516,6 +526,86 @@ void update_microsphere(Oracle& o, size_t q, double G, bool langevin = false) {
             double I = (i == j) ? Ikin[i] : 0.0;
             Dq[i * 6 + j] = (kappa + pressure) * IoI - 2.0 * pressure * I + PDP[i * 6 + j];
         }
+}
+
+// nonaffine_microsphere.cpp:29-175 (members nonaffine_microsphere.hpp: effective tube geometry
+// U = 9, tube parameter q = 1; the stretch parameter p from the material).  Chain part on the
+// non-affine stretch lambda = (sum_i w_i |t_i|^p)^(1/p), tube part on the deformed normals
+// n_i = Fbar^-T r_i (area stretch nu_i = |n_i|):
+//   h = sum w |t|^(p-2) t(x)t,  H = (p-2) sum w |t|^(p-4) t(x)t(x)t(x)t,
+//   k = q sum w nu^(q-2) n(x)n,  K = q(q-2) sum w nu^(q-4) n(x)n(x)n(x)n,
+//   G = 2q sum w nu^(q-2) o(n)   (o: compute_o_dot_product),
+//   tau = G pf lambda^(2-p) h - G N U k,
+//   C = (G ps lambda^(2-2p) - (p-1) G pf lambda^(2-2p)) h(x)h + G pf lambda^(2-p) H
+//       + G N U (K + G),
+// with pf, ps the Pade approximants at lambda; then the affine model's stress and tangent.
+void o_dot_product(const double* n, double* o6) {
+    const double n0 = n[0], n1 = n[1], n2 = n[2];
+    const double m[36] = {2.0 * n0 * n0, 0.0, 0.0, 0.0, n0 * n2, n0 * n1,
+                          0.0, 2.0 * n1 * n1, 0.0, n1 * n2, 0.0, n0 * n1,
+                          0.0, 0.0, 2.0 * n2 * n2, n1 * n2, n0 * n2, 0.0,
+                          0.0, n1 * n2, n1 * n2, 0.5 * (n1 * n1 + n2 * n2), 0.5 * n0 * n1, 0.5 * n0 * n2,
+                          n0 * n2, 0.0, n0 * n2, 0.5 * n0 * n1, 0.5 * (n0 * n0 + n2 * n2), 0.5 * n2 * n1,
+                          n0 * n1, n0 * n1, 0.0, 0.5 * n0 * n2, 0.5 * n2 * n1, 0.5 * (n0 * n0 + n1 * n1)};
+    for (int i = 0; i < 36; ++i) o6[i] = m[i];
+}
+
+void update_nonaffine(Oracle& o, size_t q, double G) {
+    const double N = o.mat.segments, p = o.mat.nonaffine_p;
+    const double U = 9.0, qt = 1.0;  // effective_tube_geometry, non_affine_tube_parameter
+    const double* Fq = &o.F[q * 9];
+    const double scale = std::pow(det3(Fq), -1.0 / 3.0);
+    double Fb[9], Fbi[9];
+    for (int i = 0; i < 9; ++i) Fb[i] = scale * Fq[i];
+    inv3(Fb, Fbi);
+    double lp = 0.0, h[9] = {0}, H[36] = {0}, k[9] = {0}, KG[36] = {0};
+    for (int i = 0; i < 21; ++i) {
+        const double* r = o.sphere.r[i];
+        const double w = o.sphere.w[i];
+        double t[3], n[3];
+        for (int a = 0; a < 3; ++a) {
+            t[a] = Fb[a * 3 + 0] * r[0] + Fb[a * 3 + 1] * r[1] + Fb[a * 3 + 2] * r[2];
+            n[a] = Fbi[0 * 3 + a] * r[0] + Fbi[1 * 3 + a] * r[1] + Fbi[2 * 3 + a] * r[2];
+        }
+        const double l = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        const double nu = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        lp += std::pow(l, p) * w;
+        double tt[9], nn[9], tv[6], nv[6], od[36];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                tt[a * 3 + b] = t[a] * t[b];
+                nn[a * 3 + b] = n[a] * n[b];
+            }
+        kinetic_voigt(tt, tv);
+        kinetic_voigt(nn, nv);
+        o_dot_product(n, od);
+        for (int a = 0; a < 9; ++a) {
+            h[a] += std::pow(l, p - 2.0) * tt[a] * w;
+            k[a] += std::pow(nu, qt - 2.0) * nn[a] * w;
+        }
+        for (int a = 0; a < 6; ++a)
+            for (int b = 0; b < 6; ++b) {
+                H[a * 6 + b] += std::pow(l, p - 4.0) * (tv[a] * tv[b]) * w;
+                KG[a * 6 + b] += qt * (qt - 2.0) * std::pow(nu, qt - 4.0) * (nv[a] * nv[b]) * w +
+                                 2.0 * qt * std::pow(nu, qt - 2.0) * od[a * 6 + b] * w;
+            }
+    }
+    const double lam = std::pow(lp, 1.0 / p);
+    for (int a = 0; a < 36; ++a) H[a] *= (p - 2.0);
+    for (int a = 0; a < 9; ++a) k[a] *= qt;
+    const double micro_tau = G * pade_first(lam, N) * lam;
+    const double micro_C = G * pade_second(lam, N);
+    double tau[9], hv[6], C[36];
+    kinetic_voigt(h, hv);
+    for (int a = 0; a < 9; ++a)
+        tau[a] = micro_tau * std::pow(lam, 1.0 - p) * h[a] - G * N * U * k[a];
+    const double chh = micro_C * std::pow(lam, 2.0 - 2.0 * p) -
+                       (p - 1.0) * micro_tau * std::pow(lam, 1.0 - 2.0 * p);
+    for (int a = 0; a < 6; ++a)
+        for (int b = 0; b < 6; ++b)
+            C[a * 6 + b] = chh * (hv[a] * hv[b]) + micro_tau * std::pow(lam, 1.0 - p) * H[a * 6 + b] +
+                           G * N * U * KG[a * 6 + b];
+    microsphere_response(o, q, tau, C);
 }
 
 // ----------------------------------------------------------------------------------------
@@ -610,6 +700,11 @@ int update_internal_variables(Oracle& o, const double* u, std::string* msg) {
             for (long long q = 0; q < (long long)nqp; ++q)
                 update_microsphere(o, (size_t)q, o.shear((int)(q / o.nq)), true);
             break;
+        case NONAFFINE_MICROSPHERE:
+#pragma omp parallel for schedule(static)
+            for (long long q = 0; q < (long long)nqp; ++q)
+                update_nonaffine(o, (size_t)q, o.shear((int)(q / o.nq)));
+            break;
     }
     if (status != ORC_OK) return status;
     // FE_INVALID check (submesh.cpp:196-207) restated as a NaN scan of the outputs
@@ -683,7 +778,7 @@ void element_stiffness(const Oracle& o, int e, double* ke) {
     }
     for (int i = 0; i < nd * nd; ++i) ke[i] = kmat[i];
     bool finite = (o.mat.model == NEO_HOOKE || o.mat.model == GAUSS_AFFINE_MICROSPHERE ||
-                   o.mat.model == LANGEVIN_AFFINE_MICROSPHERE);
+                   o.mat.model == LANGEVIN_AFFINE_MICROSPHERE || o.mat.model == NONAFFINE_MICROSPHERE);
     if (!finite) return;
     std::vector<double> kgeo(npe * npe, 0.0);
     for (int l = 0; l < nq; ++l) {
@@ -1297,6 +1392,7 @@ void* orc_create(int num_nodes, const double* coords, int num_elements, int node
     o->mat.sigma_y = params[2];
     o->mat.H_iso = params[3];
     o->mat.segments = params[4];
+    o->mat.nonaffine_p = params[5];
     if (Ge) o->Ge.assign(Ge, Ge + num_elements);
     size_t nqp = (size_t)num_elements * o->nq;
     o->H.assign(nqp * 9, 0.0);
@@ -1408,6 +1504,7 @@ int orc_constitutive_only(void* h) {
             case LANGEVIN_AFFINE_MICROSPHERE:
                 update_microsphere(*o, q, o->shear((int)(q / o->nq)), true);
                 break;
+            case NONAFFINE_MICROSPHERE: update_nonaffine(*o, q, o->shear((int)(q / o->nq))); break;
         }
     }
     return ORC_OK;

@@ -43,8 +43,9 @@ def random_displacement(mesh, scale, seed):
 
 def cube_example_problem(example: str = "neohooke_cube_example"):
     """A cube example on the shared cube mesh as a Problem: the neo-Hookean one
-    (examples/.../neohooke/cube) or, with ``affine_microsphere_cube_example``, the Langevin
-    affine microsphere one (examples/.../affine_microsphere/cube)."""
+    (examples/.../neohooke/cube), ``affine_microsphere_cube_example`` (Langevin statistics,
+    examples/.../affine_microsphere/cube) or ``nonaffine_microsphere_cube_example``
+    (examples/.../nonaffine_microsphere/cube)."""
     from neon_b200 import mesh as M
     from neon_b200 import problem as P
     with open(os.path.join(GOLDEN, "kats.json")) as fh:
@@ -60,9 +61,14 @@ def cube_example_problem(example: str = "neohooke_cube_example"):
     inc = step["time"]["increments"]
     nl = step["nonlinear_options"]
     ls = step["linear_solver"]
+    # the path's linear solver is the PCG: a deck that asks for a direct solver (PaStiX) gets
+    # the PCG at a tolerance well below the Newton tolerances instead
+    iterative = ls.get("type") == "iterative"
     opts = P.Options(residual_tolerance=nl["residual_tolerance"],
                      displacement_tolerance=nl["displacement_tolerance"],
+                     linear_iterations=nl.get("linear_iterations", 10),
                      period=step["time"]["period"], initial=inc["initial"], minimum=inc["minimum"],
                      maximum=inc["maximum"], adaptive=inc["adaptive"],
-                     cg_tolerance=ls["tolerance"], cg_maximum_iterations=ls["maximum_iterations"])
+                     cg_tolerance=ls["tolerance"] if iterative else 1e-10,
+                     cg_maximum_iterations=ls["maximum_iterations"] if iterative else 20000)
     return P.Problem(example, mesh, material, bcs, opts)

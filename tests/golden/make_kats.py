@@ -109,6 +109,19 @@ def main(ref: str):
                                               seg).group(1)),
         "uniaxial_stretch": float(re.search(r"F\(0, 0\) = ([0-9.]+);", seg).group(1)),
         "margin": 1e-5}
+    na = _find_line(lines, r'TEST_CASE\("Nonaffine microsphere"\)')
+    seg = "\n".join(lines[na:na + 100])
+    assert '\\"nonaffine\\"' in seg
+    out["nonaffine_microsphere"] = {
+        "source": f"test/hyperelastic_constitutive.cpp:{na}-{na + 98}",
+        "E": float(re.search(r'elastic_modulus\\" : ([0-9.e+-]+)', seg).group(1)),
+        "nu": float(re.search(r'poissons_ratio\\" : ([0-9.e+-]+)', seg).group(1)),
+        "nonaffine_stretch_parameter": float(
+            re.search(r'nonaffine_stretch_parameter\\":([0-9.e+-]+)', seg).group(1)),
+        "segments_per_chain": float(re.search(r'segments_per_chain\\" : ([0-9.e+-]+)',
+                                              seg).group(1)),
+        "uniaxial_stretch": float(re.search(r"F\(0, 0\) = ([0-9.]+);", seg).group(1)),
+        "margin": 1e-5}
     # --- linear solver (test/linear_solvers.cpp) --------------------------------------------
     p = os.path.join(ref, "test", "linear_solvers.cpp")
     src = open(p).read()
@@ -169,6 +182,15 @@ def main(ref: str):
     out["affine_microsphere_cube_example"] = {
         "source": "examples/solid_mechanics/hyperelastic/affine_microsphere/cube/cube.json:1-80",
         "mesh": "neohooke_cube.npz", "simulation": asim, "max_displacement": 0.5}
+    nx = os.path.join(ref, "examples", "solid_mechanics", "hyperelastic", "nonaffine_microsphere",
+                      "cube")
+    with open(os.path.join(nx, "cube.mesh"), "rb") as a, open(os.path.join(ex, "cube.mesh"),
+                                                               "rb") as b:
+        assert a.read() == b.read(), "the non-affine microsphere cube mesh differs"
+    out["nonaffine_microsphere_cube_example"] = {
+        "source": "examples/solid_mechanics/hyperelastic/nonaffine_microsphere/cube/cube.json:1-78",
+        "mesh": "neohooke_cube.npz", "simulation": json.load(open(os.path.join(nx, "cube.json"))),
+        "max_displacement": 0.5}
     with open(os.path.join(HERE, "kats.json"), "w") as fh:
         json.dump(out, fh, indent=1, sort_keys=True)
     print("wrote", os.path.join(HERE, "kats.json"))

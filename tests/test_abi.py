@@ -44,7 +44,7 @@ def test_create_rejects_bad_input_without_gpu():
     X = np.zeros((4, 3))
     conn = np.array([[0, 1, 2, 7]], np.int32)  # node 7 does not exist
     desc = api.MeshDesc(4, X.ctypes.data, 1, 4, conn.ctypes.data)
-    mat = api.MaterialDesc(0, 1.0, 1.0, 0, 0, 0)
+    mat = api.MaterialDesc(0, 1.0, 1.0, 0, 0, 0, 0)
     h = ctypes.c_void_p()
     assert L.nb2_create(ctypes.byref(desc), ctypes.byref(mat), ctypes.byref(h)) == api.E_INPUT
     buf = ctypes.create_string_buffer(256)
@@ -85,11 +85,17 @@ def test_microsphere_factory_errors():
         m = P.make_material(rubber, {**ms, "type": "affine", "quadrature": "BO21",
                                      "statistics": statistics})
         assert m.model == model and m.segments_per_chain == 50
-    with pytest.raises(NotImplementedError):  # other quadrature rules and the nonaffine model
+    with pytest.raises(NotImplementedError):  # other quadrature rules
         P.make_material(rubber, {**ms, "type": "affine", "quadrature": "FM900",
                                  "statistics": "langevin"})
-    with pytest.raises(NotImplementedError):
-        P.make_material(rubber, {**ms, "type": "nonaffine", "quadrature": "BO21"})
+    # test/hyperelastic_constitutive.cpp "Nonaffine microsphere" exception: a misspelt
+    # nonaffine_stretch_parameter
+    with pytest.raises(ValueError):
+        P.make_material({**rubber, "nonaffine_Strearameter": 1.0},
+                        {**ms, "type": "nonaffine", "quadrature": "BO21"})
+    m = P.make_material({**rubber, "nonaffine_stretch_parameter": 1.0},
+                        {**ms, "type": "nonaffine", "quadrature": "BO21"})
+    assert m.model == P.NONAFFINE_MICROSPHERE and m.nonaffine_stretch_parameter == 1.0
 
 
 def test_dirichlet_order_and_sinusoid():

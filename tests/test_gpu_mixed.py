@@ -40,9 +40,12 @@ def test_matrix_free_tangent_equals_assembled(api, topo, model):
 @pytest.mark.parametrize("make", [lambda: P.config_c1(6), lambda: P.config_c2(5, increments=3),
                                   lambda: P.config_c4(4), lambda: P.config_c5_instance(3, 1.3),
                                   lambda: P.config_c4(4, traction=0.2, statistics="langevin",
-                                                      segments_per_chain=5)],
+                                                      segments_per_chain=5),
+                                  lambda: P.config_c4(4, traction=0.2, statistics="nonaffine",
+                                                      segments_per_chain=5,
+                                                      nonaffine_stretch_parameter=1.5)],
                          ids=["c1_le_hex8", "c2_nh_hex8", "c4_microsphere_hex8", "c5_nh_tet4",
-                              "c4_langevin_hex8"])
+                              "c4_langevin_hex8", "c4_nonaffine_hex8"])
 def test_mixed_newton_reaches_fp64_solution(api, make):
     pr = make()
     pr.options.residual_tolerance = pr.options.displacement_tolerance = 1e-10

@@ -42,12 +42,16 @@ MATERIALS = {
                                  "segments_per_chain": 5},
                                 {"name": "microsphere", "type": "affine",
                                  "statistics": "langevin", "quadrature": "BO21"}),
+    "nonaffine": P.make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0,
+                                  "segments_per_chain": 5, "nonaffine_stretch_parameter": 1.5},
+                                 {"name": "microsphere", "type": "nonaffine",
+                                  "quadrature": "BO21"}),
 }
 # displacement amplitudes that keep det F > 0 and put J2 points in the plastic range
 SCALE = {"linear_elastic": 1e-3, "neohooke": 0.02, "j2": 4e-3, "microsphere": 0.02,
-         "langevin": 0.03}
+         "langevin": 0.03, "nonaffine": 0.03}
 # models with a per-element shear modulus field in the tests
-FIELD_MODELS = ("microsphere", "langevin")
+FIELD_MODELS = ("microsphere", "langevin", "nonaffine")
 
 
 def _meshes():
@@ -194,6 +198,11 @@ def _solve_both(api, oracle, pr, **kw):
                                                  segments_per_chain=5)),
     ("affine_microsphere_cube_example",
      lambda: cube_example_problem("affine_microsphere_cube_example")),
+    ("c4_nonaffine_traction", lambda: P.config_c4(4, traction=0.2, statistics="nonaffine",
+                                                  segments_per_chain=5,
+                                                  nonaffine_stretch_parameter=1.5)),
+    ("nonaffine_microsphere_cube_example",
+     lambda: cube_example_problem("nonaffine_microsphere_cube_example")),
     ("c5_neohooke_tet4", lambda: P.config_c5_instance(3, 1.3, increments=2)),
     ("neohooke_cube_example", cube_example_problem),
 ])

@@ -177,6 +177,51 @@ def test_langevin_chains_stiffen_with_stretch(oracle):
     assert ratios[5.0, 1.6] > ratios[20.0, 1.6] > 1.0
 
 
+def test_nonaffine_microsphere_known_answers(oracle, kats):
+    """test/hyperelastic_constitutive.cpp "Nonaffine microsphere": no stress and a symmetric
+    positive definite tangent at F = I, a symmetric positive definite tangent under uniaxial
+    stretch."""
+    k = kats["nonaffine_microsphere"]
+    mat = P.make_material({"elastic_modulus": k["E"], "poissons_ratio": k["nu"],
+                           "nonaffine_stretch_parameter": k["nonaffine_stretch_parameter"],
+                           "segments_per_chain": k["segments_per_chain"]},
+                          {"name": "microsphere", "type": "nonaffine", "quadrature": "BO21"})
+    assert mat.model == P.NONAFFINE_MICROSPHERE
+    om = _single_point(oracle, mat)
+    om.set("F", np.tile(np.eye(3).reshape(-1), (2, 1)))
+    om.set("detF", np.ones(2))
+    om.constitutive_only()
+    assert all(_is_spd(D) for D in om.get("D"))
+    assert np.abs(om.get("sigma")).max() / mat.G < 1e-5
+    _uniaxial(om, k["uniaxial_stretch"])
+    assert all(_is_spd(D) for D in om.get("D"))
+    assert all(np.linalg.norm(s) > 0 for s in om.get("sigma"))
+
+
+def test_nonaffine_stress_is_objective_and_isochoric(oracle):
+    """The non-affine model depends on F only through Fbar, and through Fbar by stretches:
+    a rotation R F gives R sigma R^T, a dilatation leaves the deviatoric stress unchanged."""
+    mat = P.make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0,
+                           "nonaffine_stretch_parameter": 1.0, "segments_per_chain": 50},
+                          {"name": "microsphere", "type": "nonaffine", "quadrature": "BO21"})
+    F = np.array([[1.2, 0.1, 0.0], [0.05, 0.9, 0.1], [0.0, -0.1, 1.05]])
+    c, s_ = np.cos(0.4), np.sin(0.4)
+    R = np.array([[c, -s_, 0], [s_, c, 0], [0, 0, 1.0]])
+    out = {}
+    for key, Fq in (("F", F), ("RF", R @ F), ("aF", 1.1 * F)):
+        om = _single_point(oracle, mat)
+        om.set("F", np.tile(Fq.reshape(-1), (2, 1)))
+        om.set("detF", np.full(2, np.linalg.det(Fq)))
+        om.constitutive_only()
+        out[key] = om.get("sigma")[0].reshape(3, 3)
+    scale = np.abs(out["F"]).max()
+    assert np.abs(R @ out["F"] @ R.T - out["RF"]).max() < 1e-12 * scale
+    dev = lambda s: s - np.trace(s) / 3 * np.eye(3)  # noqa: E731
+    # the deviatoric Kirchhoff stress J dev(sigma) is the same for F and a F
+    assert np.abs(np.linalg.det(F) * dev(out["F"]) -
+                  np.linalg.det(1.1 * F) * dev(out["aF"])).max() < 1e-12 * scale
+
+
 def test_langevin_cube_example_deck(kats):
     """The affine microsphere cube example's deck builds the Langevin model on the shared cube
     mesh (examples/.../affine_microsphere/cube/cube.json)."""
@@ -184,6 +229,9 @@ def test_langevin_cube_example_deck(kats):
     assert pr.material.model == P.LANGEVIN_AFFINE_MICROSPHERE
     assert pr.material.segments_per_chain == 45
     assert pr.mesh.conn.shape[1] == 8
+    pn = cube_example_problem("nonaffine_microsphere_cube_example")
+    assert pn.material.model == P.NONAFFINE_MICROSPHERE
+    assert pn.material.nonaffine_stretch_parameter == 1.0 and pn.options.linear_iterations == 15
 
 
 def test_cg_three_by_three(oracle, kats):
