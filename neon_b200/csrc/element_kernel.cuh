@@ -14,7 +14,7 @@
 #pragma once
 
 template <int NPE, int MODEL, typename Real, int MODE>
-__global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : (model_aniso(MODEL) ? 4 : 8))
+__global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MODEL) ? 4 : 8))
     k_element(ElementArgs A) {
     using T = Topo<NPE>;
     constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC, MAXB = T::MAXB;
@@ -29,6 +29,9 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : (model_aniso(MOD
     constexpr int NS = kJ2 ? NQ * 6 + 2 : (kAniso ? NQ * 21 + 2 : 1);  // N or s Da
     constexpr int GS = kFinite ? NQ * NPE * 3 + 1 : 1;  // g = s sigma L
     constexpr int NG = (NPE + G - 1) / G;          // nodes per lane
+    // hex8 FP64 blocks on the FP64 mma.sync path (the anisotropic microsphere tangent keeps the
+    // per-lane block loop)
+    constexpr bool kMmaBlocks = (NPE == 8) && (sizeof(Real) == 8) && !kAniso;
 
     __shared__ double sX[EPC][NPE][3];
     __shared__ double sx[EPC][NPE][3];
@@ -37,6 +40,11 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : (model_aniso(MOD
     __shared__ Real sN[EPC][NS];
     __shared__ double sG[EPC][GS];
     __shared__ Real sC[EPC][NQ][4];
+    // mma path: one element's 64 blocks and their slots per warp, staged so that consecutive
+    // lanes reduce consecutive entries of a block (72 contiguous bytes in K)
+    constexpr int KS = kMmaBlocks ? NPE * NPE * 9 : 1;
+    __shared__ double sKe[kMmaBlocks ? 2 : 1][KS];
+    __shared__ int sSl[kMmaBlocks ? 2 : 1][kMmaBlocks ? NPE * NPE : 1];
 
     const int tid = threadIdx.x;
     const int le = tid / G;
@@ -226,19 +234,117 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 6 : (model_aniso(MOD
         }
     }
     __syncthreads();
-    if (!valid) return;
 
     if constexpr (kForce) {
+        if (valid) {
 #pragma unroll
-        for (int j = 0; j < NG; ++j) {
-            const int a = lane + j * G;
-            if (a < NPE) {
-                atomicAdd(&A.fint[3ll * node[j] + 0], fown[j][0]);
-                atomicAdd(&A.fint[3ll * node[j] + 1], fown[j][1]);
-                atomicAdd(&A.fint[3ll * node[j] + 2], fown[j][2]);
+            for (int j = 0; j < NG; ++j) {
+                const int a = lane + j * G;
+                if (a < NPE) {
+                    atomicAdd(&A.fint[3ll * node[j] + 0], fown[j][0]);
+                    atomicAdd(&A.fint[3ll * node[j] + 1], fown[j][1]);
+                    atomicAdd(&A.fint[3ll * node[j] + 2], fown[j][2]);
+                }
             }
         }
     }
+
+    if constexpr (kStiff && kMmaBlocks) {
+        // hex8 FP64: each warp forms the 64 blocks of its 4 elements, one element at a time,
+        // as 8x8 (node x node) products over the 8 points with mma.sync m8n8k4 (FP64).  Lane
+        // (g, t) = (lane / 4, lane % 4) supplies the A operand (node g, point t + 4s) and the B
+        // operand (point t + 4s, node g) of k-step s from the same shared values, and receives
+        // the blocks (g, 2t) and (g, 2t + 1):
+        //   K^ik = sum_q (s lam' L_qi)(L_qk)^T + (s mu' L_qk)(L_qi)^T
+        //          + [i == k] sum_q sum_m (s mu' L_qm + s (sigma L)_qm)(L_qm)^T
+        //          + sum_q (s b (N L)_qi)(N L)_qk^T                      (plastic J2 points)
+        // -- the block formula above with both triangles formed, so no mirrored scatter.
+        const int lane32 = tid & 31, warp = tid >> 5;
+        const int g = lane32 >> 2, t = lane32 & 3;
+        double* Kp = reinterpret_cast<double*>(A.K64);
+#pragma unroll 1
+        for (int j = 0; j < 4; ++j) {
+            const int le2 = warp * 4 + j;
+            const long long e2 = (long long)blockIdx.x * EPC + le2;
+            if (!element_enabled(A, e2)) continue;  // the same for all lanes of the warp
+            double Lq[2][3], cl[2], cm[2], cb[2];
+#pragma unroll
+            for (int st = 0; st < 2; ++st) {
+                const int q = t + 4 * st;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) Lq[st][k] = (double)sL[le2][q * NPE * 3 + 3 * g + k];
+                cl[st] = (double)sC[le2][q][0];
+                cm[st] = (double)sC[le2][q][1];
+                cb[st] = (double)sC[le2][q][2];
+            }
+            double acc[9][2];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) acc[c][0] = acc[c][1] = 0.0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+#pragma unroll
+                    for (int st = 0; st < 2; ++st) {
+                        dmma_8x8x4(acc[3 * i + k], cl[st] * Lq[st][i], Lq[st][k]);
+                        dmma_8x8x4(acc[3 * i + k], cm[st] * Lq[st][k], Lq[st][i]);
+                    }
+            double sd[2] = {0.0, 0.0};
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+#pragma unroll
+                for (int st = 0; st < 2; ++st) {
+                    double av = cm[st] * Lq[st][m];
+                    if constexpr (kFinite) av += sG[le2][(t + 4 * st) * NPE * 3 + 3 * g + m];
+                    dmma_8x8x4(sd, av, Lq[st][m]);
+                }
+            if constexpr (kJ2) {
+                if (__any_sync(0xffffffffu, cb[0] != 0.0 || cb[1] != 0.0)) {
+                    double V[2][3];
+#pragma unroll
+                    for (int st = 0; st < 2; ++st) {
+                        const Real* Nq = &sN[le2][(t + 4 * st) * 6];
+                        const double N0 = Nq[0], N1 = Nq[1], N2 = Nq[2], N3 = Nq[3], N4 = Nq[4],
+                                     N5 = Nq[5];
+                        V[st][0] = N0 * Lq[st][0] + N5 * Lq[st][1] + N4 * Lq[st][2];
+                        V[st][1] = N5 * Lq[st][0] + N1 * Lq[st][1] + N3 * Lq[st][2];
+                        V[st][2] = N4 * Lq[st][0] + N3 * Lq[st][1] + N2 * Lq[st][2];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+#pragma unroll
+                            for (int st = 0; st < 2; ++st)
+                                dmma_8x8x4(acc[3 * i + k], cb[st] * V[st][i], V[st][k]);
+                }
+            }
+            const int* slot = A.slot + e2 * (NPE * NPE);
+            sSl[warp][lane32] = slot[lane32];
+            sSl[warp][32 + lane32] = slot[32 + lane32];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                acc[0][c] += sd[c];
+                acc[4][c] += sd[c];
+                acc[8][c] += sd[c];
+                const int blk = g * NPE + 2 * t + c;
+#pragma unroll
+                for (int i = 0; i < 9; ++i) sKe[warp][blk * 9 + i] = acc[i][c];
+            }
+            __syncwarp();
+#pragma unroll 6
+            for (int it = 0; it < NPE * NPE * 9 / 32; ++it) {
+                const int idx = it * 32 + lane32;
+                const int blk = idx / 9;
+                const long long sab = sSl[warp][blk];
+                atomicAdd(&Kp[9 * sab + (idx - 9 * blk)], sKe[warp][idx]);
+            }
+            __syncwarp();
+        }
+        return;
+    }
+
+    if (!valid) return;
 
     if constexpr (kStiff) {
         const int* seg = (NPE == 8) ? c_seg_hex8[lane] : c_seg_tet4[lane];

@@ -501,6 +501,14 @@ __device__ __forceinline__ bool element_enabled(const ElementArgs& A, long long 
     return e < A.E && (A.inst_on == nullptr || A.inst_on[A.e_inst[e]] != 0);
 }
 
+// D += A B for one 8x8x4 FP64 tile (mma.sync m8n8k4, row.col): lane l holds A[l/4][l%4],
+// B[l%4][l/4] and D[l/4][2(l%4) + {0, 1}]
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
 #include "element_kernel.cuh"
 
 // ---------------------------------------------------------------------------------------
