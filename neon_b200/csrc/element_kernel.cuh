@@ -42,7 +42,8 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
     __shared__ Real sC[EPC][NQ][4];
     // mma path: one element's 64 blocks and their slots per warp, staged so that consecutive
     // lanes reduce consecutive entries of a block (72 contiguous bytes in K)
-    constexpr int KS = kMmaBlocks ? NPE * NPE * 9 : 1;
+    // (one padding double per 16 blocks: the 16 lanes of a half-warp write distinct banks)
+    constexpr int KS = kMmaBlocks ? NPE * NPE * 9 + 4 : 1;
     __shared__ double sKe[kMmaBlocks ? 2 : 1][KS];
     __shared__ int sSl[kMmaBlocks ? 2 : 1][kMmaBlocks ? NPE * NPE : 1];
 
@@ -267,6 +268,8 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
             const int le2 = warp * 4 + j;
             const long long e2 = (long long)blockIdx.x * EPC + le2;
             if (!element_enabled(A, e2)) continue;  // the same for all lanes of the warp
+            const int* slot = A.slot + e2 * (NPE * NPE);
+            const int sl0 = slot[lane32], sl1 = slot[32 + lane32];
             double Lq[2][3], cl[2], cm[2], cb[2];
 #pragma unroll
             for (int st = 0; st < 2; ++st) {
@@ -319,9 +322,8 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                                 dmma_8x8x4(acc[3 * i + k], cb[st] * V[st][i], V[st][k]);
                 }
             }
-            const int* slot = A.slot + e2 * (NPE * NPE);
-            sSl[warp][lane32] = slot[lane32];
-            sSl[warp][32 + lane32] = slot[32 + lane32];
+            sSl[warp][lane32] = sl0;
+            sSl[warp][32 + lane32] = sl1;
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 acc[0][c] += sd[c];
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                 acc[8][c] += sd[c];
                 const int blk = g * NPE + 2 * t + c;
 #pragma unroll
-                for (int i = 0; i < 9; ++i) sKe[warp][blk * 9 + i] = acc[i][c];
+                for (int i = 0; i < 9; ++i) sKe[warp][blk * 9 + i + (blk >> 4)] = acc[i][c];
             }
             __syncwarp();
 #pragma unroll 6
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                 const int idx = it * 32 + lane32;
                 const int blk = idx / 9;
                 const long long sab = sSl[warp][blk];
-                atomicAdd(&Kp[9 * sab + (idx - 9 * blk)], sKe[warp][idx]);
+                atomicAdd(&Kp[9 * sab + (idx - 9 * blk)], sKe[warp][idx + (blk >> 4)]);
             }
             __syncwarp();
         }
