@@ -35,7 +35,8 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
 
     __shared__ double sX[EPC][NPE][3];
     __shared__ double sx[EPC][NPE][3];
-    __shared__ double sdN[NQ][NPE][3];
+    // one padding node per point: the 8 points' rows (27 doubles apart) fall on distinct banks
+    __shared__ double sdN[NQ][NPE + 1][3];
     __shared__ Real sL[EPC][LS];
     __shared__ Real sN[EPC][NS];
     __shared__ double sG[EPC][GS];
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
     const bool valid = element_enabled(A, e);
 
     for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
-        (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
+        sdN[i / (NPE * 3)][(i % (NPE * 3)) / 3][i % 3] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
 
     // phase 0
     int node[NG];
