@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
         //   K^ik = sum_q (s lam' L_qi)(L_qk)^T + (s mu' L_qk)(L_qi)^T
         //          + [i == k] sum_q sum_m (s mu' L_qm + s (sigma L)_qm)(L_qm)^T
         //          + sum_q (s b (N L)_qi)(N L)_qk^T                      (plastic J2 points)
-        // -- the block formula above with both triangles formed, so no mirrored scatter.
+        // -- the block formula above, all 64 blocks of the element, so no mirrored scatter.
         const int lane32 = tid & 31, warp = tid >> 5;
         const int g = lane32 >> 2, t = lane32 & 3;
         double* Kp = reinterpret_cast<double*>(A.K64);
@@ -281,17 +281,26 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                 cm[st] = (double)sC[le2][q][1];
                 cb[st] = (double)sC[le2][q][2];
             }
-            double acc[9][2];
+            // K is symmetric (K_ba[k][i] = K_ab[i][k]): only the component tiles i <= k are
+            // formed; the diagonal ones merge their two products, and the staging writes each
+            // off-diagonal value into both of its places
+            constexpr int kTile[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+            double acc[6][2];
 #pragma unroll
-            for (int c = 0; c < 9; ++c) acc[c][0] = acc[c][1] = 0.0;
+            for (int c = 0; c < 6; ++c) acc[c][0] = acc[c][1] = 0.0;
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int k = 0; k < 3; ++k)
+                for (int st = 0; st < 2; ++st)
+                    dmma_8x8x4(acc[kTile[i][i]], (cl[st] + cm[st]) * Lq[st][i], Lq[st][i]);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = i + 1; k < 3; ++k)
 #pragma unroll
                     for (int st = 0; st < 2; ++st) {
-                        dmma_8x8x4(acc[3 * i + k], cl[st] * Lq[st][i], Lq[st][k]);
-                        dmma_8x8x4(acc[3 * i + k], cm[st] * Lq[st][k], Lq[st][i]);
+                        dmma_8x8x4(acc[kTile[i][k]], cl[st] * Lq[st][i], Lq[st][k]);
+                        dmma_8x8x4(acc[kTile[i][k]], cm[st] * Lq[st][k], Lq[st][i]);
                     }
             double sd[2] = {0.0, 0.0};
 #pragma unroll
@@ -317,22 +326,29 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
 #pragma unroll
                     for (int i = 0; i < 3; ++i)
 #pragma unroll
-                        for (int k = 0; k < 3; ++k)
+                        for (int k = i; k < 3; ++k)
 #pragma unroll
                             for (int st = 0; st < 2; ++st)
-                                dmma_8x8x4(acc[3 * i + k], cb[st] * V[st][i], V[st][k]);
+                                dmma_8x8x4(acc[kTile[i][k]], cb[st] * V[st][i], V[st][k]);
                 }
             }
             sSl[warp][lane32] = sl0;
             sSl[warp][32 + lane32] = sl1;
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
-                acc[0][c] += sd[c];
-                acc[4][c] += sd[c];
-                acc[8][c] += sd[c];
-                const int blk = g * NPE + 2 * t + c;
+                const int b = 2 * t + c;
+                const int blk = g * NPE + b, blkT = b * NPE + g;
+                double* Kab = &sKe[warp][blk * 9 + (blk >> 4)];
+                double* Kba = &sKe[warp][blkT * 9 + (blkT >> 4)];
 #pragma unroll
-                for (int i = 0; i < 9; ++i) sKe[warp][blk * 9 + i + (blk >> 4)] = acc[i][c];
+                for (int i = 0; i < 3; ++i) {
+                    Kab[4 * i] = acc[kTile[i][i]][c] + sd[c];
+#pragma unroll
+                    for (int k = i + 1; k < 3; ++k) {
+                        Kab[3 * i + k] = acc[kTile[i][k]][c];
+                        Kba[3 * k + i] = acc[kTile[i][k]][c];
+                    }
+                }
             }
             __syncwarp();
 #pragma unroll 6
