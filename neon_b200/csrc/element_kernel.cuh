@@ -180,8 +180,8 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
             s = w * det3(Fc);
         }
         if constexpr (kStiff || kForce) {
-#pragma unroll
-            for (int a = 0; a < NPE; ++a) {
+            // per node a: L_a = J^-T dN_a (stored for the stiffness phase) and g_a = s sigma L_a
+            auto node_terms = [&](int a, double (&gv)[3]) {
                 double La[3] = {0.0, 0.0, 0.0};
                 if (active) {
 #pragma unroll
@@ -189,33 +189,73 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                         La[k] = sdN[l][a][0] * Ji[0 * 3 + k] + sdN[l][a][1] * Ji[1 * 3 + k] +
                                 sdN[l][a][2] * Ji[2 * 3 + k];
                 }
-                // g_a = s sigma L_a (sigma symmetric: 11 22 33 23 13 12)
-                double g0 = s * (o.sig[0] * La[0] + o.sig[5] * La[1] + o.sig[4] * La[2]);
-                double g1 = s * (o.sig[5] * La[0] + o.sig[1] * La[1] + o.sig[3] * La[2]);
-                double g2 = s * (o.sig[4] * La[0] + o.sig[3] * La[1] + o.sig[2] * La[2]);
+                // sigma symmetric: 11 22 33 23 13 12
+                gv[0] = s * (o.sig[0] * La[0] + o.sig[5] * La[1] + o.sig[4] * La[2]);
+                gv[1] = s * (o.sig[5] * La[0] + o.sig[1] * La[1] + o.sig[3] * La[2]);
+                gv[2] = s * (o.sig[4] * La[0] + o.sig[3] * La[1] + o.sig[2] * La[2]);
                 if (active) {
                     if constexpr (kStiff) {
 #pragma unroll
                         for (int k = 0; k < 3; ++k) sL[le][l * NPE * 3 + 3 * a + k] = (Real)La[k];
                     }
                     if constexpr (kFinite && kStiff) {
-                        sG[le][l * NPE * 3 + 3 * a + 0] = g0;
-                        sG[le][l * NPE * 3 + 3 * a + 1] = g1;
-                        sG[le][l * NPE * 3 + 3 * a + 2] = g2;
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) sG[le][l * NPE * 3 + 3 * a + k] = gv[k];
                     }
                 }
-                if constexpr (kForce) {
-                    // sum over the group's points (inactive lanes contribute zero)
+            };
+            if constexpr (NPE == 8 && G == 8 && kForce) {
+                // internal force: a reduce-scatter over the 8 points of the group.  Each xor
+                // round sends the half of the partial sums that the partner keeps, so lane l
+                // ends with node l's sum (21 FP64 shuffles instead of 72); the additions are the
+                // same tree as a full butterfly per node (own partial + partner's partial)
+                const bool b2 = (lane & 4) != 0, b1 = (lane & 2) != 0, b0 = (lane & 1) != 0;
+                double k1[4][3];
 #pragma unroll
-                    for (int off = G / 2; off > 0; off >>= 1) {
-                        g0 += __shfl_xor_sync(0xffffffffu, g0, off);
-                        g1 += __shfl_xor_sync(0xffffffffu, g1, off);
-                        g2 += __shfl_xor_sync(0xffffffffu, g2, off);
+                for (int p = 0; p < 4; ++p) {
+                    double gl[3], gu[3];
+                    node_terms(p, gl);
+                    node_terms(p + 4, gu);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const double recv = __shfl_xor_sync(0xffffffffu, b2 ? gl[c] : gu[c], 4);
+                        k1[p][c] = (b2 ? gu[c] : gl[c]) + recv;
                     }
-                    if (a % G == lane) {
-                        fown[a / G][0] = g0;
-                        fown[a / G][1] = g1;
-                        fown[a / G][2] = g2;
+                }
+                double k2[2][3];
+#pragma unroll
+                for (int p = 0; p < 2; ++p)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const double x = k1[p][c], y = k1[p + 2][c];
+                        const double recv = __shfl_xor_sync(0xffffffffu, b1 ? x : y, 2);
+                        k2[p][c] = (b1 ? y : x) + recv;
+                    }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const double x = k2[0][c], y = k2[1][c];
+                    const double recv = __shfl_xor_sync(0xffffffffu, b0 ? x : y, 1);
+                    fown[0][c] = (b0 ? y : x) + recv;
+                }
+            } else {
+#pragma unroll
+                for (int a = 0; a < NPE; ++a) {
+                    double gv[3];
+                    node_terms(a, gv);
+                    double g0 = gv[0], g1 = gv[1], g2 = gv[2];
+                    if constexpr (kForce) {
+                        // sum over the group's points (inactive lanes contribute zero)
+#pragma unroll
+                        for (int off = G / 2; off > 0; off >>= 1) {
+                            g0 += __shfl_xor_sync(0xffffffffu, g0, off);
+                            g1 += __shfl_xor_sync(0xffffffffu, g1, off);
+                            g2 += __shfl_xor_sync(0xffffffffu, g2, off);
+                        }
+                        if (a % G == lane) {
+                            fown[a / G][0] = g0;
+                            fown[a / G][1] = g1;
+                            fown[a / G][2] = g2;
+                        }
                     }
                 }
             }
