@@ -33,20 +33,28 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
     // per-lane block loop)
     constexpr bool kMmaBlocks = (NPE == 8) && (sizeof(Real) == 8) && !kAniso;
 
-    __shared__ double sX[EPC][NPE][3];
-    __shared__ double sx[EPC][NPE][3];
-    // one padding node per point: the 8 points' rows (27 doubles apart) fall on distinct banks
-    __shared__ double sdN[NQ][NPE + 1][3];
+    // phases 0-1 only: node coordinates and the reference gradients (one padding node per
+    // point: the 8 points' rows, 27 doubles apart, fall on distinct banks)
+    using XT = double[EPC][NPE][3];
+    using DNT = double[NQ][NPE + 1][3];
+    // mma path, phase 2 only: one element's 64 blocks per warp, staged so that consecutive lanes
+    // reduce consecutive entries of a block (72 contiguous bytes in K); one padding double per
+    // 16 blocks so that the 16 lanes of a half-warp write distinct banks.  It overlays the
+    // phase 0-1 arrays: a barrier separates the two uses.
+    constexpr int KS = kMmaBlocks ? NPE * NPE * 9 + 4 : 1;
+    using KT = double[kMmaBlocks ? 2 : 1][KS];
+    constexpr size_t kP01 = 2 * sizeof(XT) + sizeof(DNT);
+    constexpr size_t kRaw = kP01 > sizeof(KT) ? kP01 : sizeof(KT);
+    __shared__ __align__(16) unsigned char sRaw[kRaw];
+    XT& sX = *reinterpret_cast<XT*>(sRaw);
+    XT& sx = *reinterpret_cast<XT*>(sRaw + sizeof(XT));
+    DNT& sdN = *reinterpret_cast<DNT*>(sRaw + 2 * sizeof(XT));
+    KT& sKe = *reinterpret_cast<KT*>(sRaw);
     __shared__ Real sL[EPC][LS];
     __shared__ Real sN[EPC][NS];
     __shared__ double sG[EPC][GS];
     __shared__ Real sC[EPC][NQ][4];
-    // mma path: one element's 64 blocks and their slots per warp, staged so that consecutive
-    // lanes reduce consecutive entries of a block (72 contiguous bytes in K)
-    // (one padding double per 16 blocks: the 16 lanes of a half-warp write distinct banks)
-    constexpr int KS = kMmaBlocks ? NPE * NPE * 9 + 4 : 1;
-    __shared__ double sKe[kMmaBlocks ? 2 : 1][KS];
-    __shared__ int sSl[kMmaBlocks ? 2 : 1][kMmaBlocks ? NPE * NPE : 1];
+    __shared__ int sSl[kMmaBlocks ? 2 : 1][kMmaBlocks ? NPE * NPE : 1];  // the staged blocks' slots
 
     const int tid = threadIdx.x;
     const int le = tid / G;
