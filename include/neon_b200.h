@@ -125,7 +125,8 @@ typedef struct nb2_solve_report {
     int32_t load_steps;
     int64_t newton_iterations;
     int64_t cg_iterations;
-    double seconds_total;
+    double seconds_total;           /* wall time of the load stepping, after the context's
+                                       solver buffers are set up (once per context) */
     double seconds_update_assembly; /* device time of the element kernels */
     double seconds_solve;           /* device time of the linear solves */
     char message[256];

@@ -196,6 +196,7 @@ int cuda_fail(nb2_ctx* c, cudaError_t e, const char* what);
 // api.cu: lazily allocated buffers and the element status word
 int ensure_k64(nb2_ctx* c);            // K64
 int ensure_k32(nb2_ctx* c);            // K32 and the FP32 CG vectors
+int ensure_cg32(nb2_ctx* c);           // the FP32 CG vectors only (matrix-free mixed PCG)
 int ensure_split_buffers(nb2_ctx* c);  // stored quadrature-point outputs + their displacement
 int reset_status(nb2_ctx* c);
 int read_status(nb2_ctx* c);           // synchronises; the status code + neon's message
