@@ -34,6 +34,11 @@ constexpr int kBatchChunk = 32;  // CG iterations per captured graph
 constexpr int kModeK64 = 0;    // FP64 K, FP64 vectors
 constexpr int kModeK32V64 = 1; // FP32 K, FP64 vectors (the batched mixed path)
 
+// a cycle of the mixed reliable-update PCG whose FP32 recurrence residual has grown to this
+// multiple of its squared norm at the residual replacement has diverged (CG residual norms are
+// not monotone, so the margin is wide: a factor 1000 in the norm)
+constexpr double kCycleDivergence = 1e6;
+
 struct Tables {
     const int* row0;   // [nchunks] first block row
     const int* row1;   // [nchunks] one past the last
@@ -45,6 +50,7 @@ struct Tables {
 // per-instance PCG scalars, structure of arrays of length ninst
 struct Scalars {
     double *rhs2, *thr, *absnew, *pq, *alpha, *rr, *beta;
+    double* rrcap;     // recurrence residual above which a reliable-update cycle has diverged
     int *iters, *done, *status, *maxit;
     unsigned* ticket;  // [4][ninst]
     int ninst;
@@ -130,6 +136,7 @@ __global__ void __launch_bounds__(kThreads) k_b_init(Tables T, const double* __r
             S.rhs2[inst] = tot[0];
             S.thr[inst] = fmax(tol * tol * tot[0], DBL_MIN);
             S.rr[inst] = tot[1];
+            S.rrcap[inst] = INFINITY;
             S.absnew[inst] = tot[2];
             S.iters[inst] = 0;
             S.status[inst] = 0;
@@ -224,6 +231,9 @@ __global__ void __launch_bounds__(kThreads) k_b_xr(Tables T, X* x, X* r, const X
                 S.status[inst] = NB2_E_NAN;
             } else if (tot[0] < S.thr[inst]) {
                 S.done[inst] = 1;
+            } else if (tot[0] > S.rrcap[inst]) {
+                S.done[inst] = 1;
+                S.status[inst] = NB2_E_CG_BREAKDOWN;
             } else {
                 S.beta[inst] = tot[1] / S.absnew[inst];
                 S.absnew[inst] = tot[1];
@@ -398,11 +408,21 @@ __global__ void __launch_bounds__(kThreads) k_b_true_residual(Tables T, const in
         if (threadIdx.x == 0) {
             rr_out[inst] = tot[0];
             S.rr[inst] = tot[0];
+            S.rrcap[inst] = kCycleDivergence * tot[0];
             S.beta[inst] = tot[1] / S.absnew[inst];
             S.absnew[inst] = tot[1];
             S.ticket[3 * S.ninst + inst] = 0;
         }
     }
+}
+
+// restart the flagged instances' cycle from the replaced residual with a fresh search
+// direction (beta = 0) and a cleared status
+__global__ void k_b_restart_cycle(int ninst, const int* flag, Scalars S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ninst || !flag[i]) return;
+    S.beta[i] = 0.0;
+    S.status[i] = NB2_OK;
 }
 
 unsigned vgrid(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148 * 8); }
@@ -428,7 +448,7 @@ struct BatchState {
     int ninst = 0, nchunks = 0, rows = 32, lanes = 16;
     std::vector<int> h_first, h_count, h_node_off;
     int *row0 = nullptr, *row1 = nullptr, *inst = nullptr, *first = nullptr, *count = nullptr;
-    double* dbuf = nullptr;    // 7 x ninst
+    double* dbuf = nullptr;    // 8 x ninst
     int* ibuf = nullptr;       // 4 x ninst
     unsigned* tickets = nullptr;
     double* part = nullptr;    // 5 x nchunks
@@ -450,6 +470,7 @@ struct BatchState {
         S.alpha = dbuf + 4 * n;
         S.rr = dbuf + 5 * n;
         S.beta = dbuf + 6 * n;
+        S.rrcap = dbuf + 7 * n;
         S.iters = ibuf;
         S.done = ibuf + n;
         S.status = ibuf + 2 * n;
@@ -513,7 +534,7 @@ int batch_setup(nb2_ctx* c, const int* node_offsets, int ninst, int R, int lanes
     if (e == cudaSuccess) e = upload(&b->inst, in);
     if (e == cudaSuccess) e = upload(&b->first, b->h_first);
     if (e == cudaSuccess) e = upload(&b->count, b->h_count);
-    if (e == cudaSuccess) e = cudaMalloc(&b->dbuf, sizeof(double) * 7 * ninst);
+    if (e == cudaSuccess) e = cudaMalloc(&b->dbuf, sizeof(double) * 8 * ninst);
     if (e == cudaSuccess) e = cudaMalloc(&b->ibuf, sizeof(int) * 4 * ninst);
     if (e == cudaSuccess) e = cudaMalloc(&b->tickets, sizeof(unsigned) * 4 * ninst);
     if (e == cudaSuccess) e = cudaMalloc(&b->part, sizeof(double) * 5 * b->nchunks);
@@ -844,7 +865,7 @@ struct BatchNewton {
         NB2_CUDA(c, cudaMemcpyAsync(thr.data(), S.thr, sizeof(double) * ninst,
                                     cudaMemcpyDeviceToHost, c->stream));
         NB2_CUDA(c, cudaStreamSynchronize(c->stream));
-        std::vector<int> finished(ninst), paused(ninst), done(ninst);
+        std::vector<int> finished(ninst), paused(ninst), done(ninst), fresh_p(ninst), resets(ninst);
         for (int i = 0; i < ninst; ++i) {
             thr_final[i] = std::max(tol * tol * b2[i], DBL_MIN);
             finished[i] = !solving[i] || b2[i] == 0.0;
@@ -855,12 +876,23 @@ struct BatchNewton {
             NB2_TRY(batch_pcg_iterate(c, b, kModeK32V64, maxit, o.use_graphs != 0));
             for (int i = 0; i < ninst; ++i) {
                 paused[i] = 0;
+                fresh_p[i] = 0;
                 if (finished[i]) continue;
                 its[i] = b->h_iters[i];
                 const int s = b->h_status[i];
-                if (s != NB2_OK && s != NB2_E_CG_MAXIT) {
+                if (s == NB2_E_CG_BREAKDOWN && resets[i] < 3) {
+                    // the cycle diverged (its retained search direction no longer fits the
+                    // replaced residual): replace the residual again and restart the cycle
+                    // with p = M^-1 r
+                    ++resets[i];
+                    fresh_p[i] = 1;
+                    paused[i] = 1;
+                } else if (s != NB2_OK && s != NB2_E_CG_MAXIT) {
                     st[i] = s;
                     finished[i] = 1;
+                    if (std::getenv("NB2_DEBUG"))
+                        std::fprintf(stderr, "[nb2] batch mixed CG: instance %d status %d after %d "
+                                     "iterations (reliable update %d)\n", i, s, its[i], update);
                 } else {
                     paused[i] = 1;
                 }
@@ -913,6 +945,11 @@ struct BatchNewton {
                                         cudaMemcpyHostToDevice, c->stream));
             NB2_CUDA(c, cudaMemcpyAsync(S.done, done.data(), sizeof(int) * ninst,
                                         cudaMemcpyHostToDevice, c->stream));
+            if (any(fresh_p)) {
+                NB2_TRY(upload_flags(c, b->flag_b, fresh_p));
+                k_b_restart_cycle<<<(ninst + 255) / 256, 256, 0, c->stream>>>(ninst, b->flag_b, S);
+                c->launches++;
+            }
             k_b_p<double><<<b->nchunks, kThreads, 0, c->stream>>>(T, c->cg_p, c->cg_r, c->cg_inv,
                                                                   S);
             c->launches++;
