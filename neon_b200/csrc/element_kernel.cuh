@@ -4,13 +4,18 @@
 //   phase 0  gather node coordinates (X, x = u + X) into shared memory;
 //   phase 1  lane l runs quadrature point l in FP64 (deformation measures, det F check,
 //            constitutive update, current gradient L = dN J^-1, tangent coefficients); the
-//            internal force of every node is reduced over the group with shuffles;
-//   phase 2  each lane accumulates its upper-triangular 3x3 blocks over the points in Real
-//            precision, in two passes of at most 3 blocks (fewer live registers), and adds
-//            them (and their mirrored blocks) to K with red.global.add.
+//            internal force of every node is reduced over the group with shuffles (hex8: a
+//            reduce-scatter, so lane l ends with node l's force);
+//   phase 2  hex8 in FP64 (every model but the anisotropic microspheres): each warp forms the
+//            64 blocks of its elements, one element at a time, as 8x8 node x node tiles with
+//            FP64 mma.sync, stages them in shared memory and adds them to K with red.global.add,
+//            consecutive lanes on consecutive entries of a block;
+//            otherwise: each lane accumulates its upper-triangular 3x3 blocks over the points in
+//            Real precision, in passes of at most 3 blocks (fewer live registers), and adds them
+//            (and their mirrored blocks) to K with red.global.add.
 // Shared memory per element holds L (Real) for every point, the flow direction N (J2) or the
-// anisotropic tangent s Da (Langevin and non-affine microsphere) and, for finite-strain models, g = s sigma L
-// (FP64) used by the geometric stiffness.
+// anisotropic tangent s Da (Langevin and non-affine microsphere) and, for finite-strain models,
+// g = s sigma L (FP64) used by the geometric stiffness.
 #pragma once
 
 template <int NPE, int MODEL, typename Real, int MODE>
