@@ -90,6 +90,7 @@ struct ElementArgs {
 struct CgScalars {
     double rhs_norm2, threshold;
     double abs_new, pq, alpha, rr, rz, beta;
+    double rr_cap;  // mixed reliable updates: recurrence r.r above which a cycle has diverged
     int iterations, max_iterations, done, status;
     unsigned int counter[4];  // last-block tickets of the reductions
 };

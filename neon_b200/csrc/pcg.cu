@@ -303,6 +303,9 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(long long n, X* __restrict__
             s->rr = tot[0];
             if (tot[0] < s->threshold) {
                 s->done = 1;
+            } else if (tot[0] > s->rr_cap) {
+                s->done = 1;
+                s->status = NB2_E_CG_BREAKDOWN;
             } else {
                 s->beta = tot[1] / s->abs_new;
                 s->abs_new = tot[1];
@@ -373,6 +376,7 @@ __global__ void __launch_bounds__(kRedThreads) k_init(long long n, const double*
             s->rr = tot[1];
             s->abs_new = tot[2];
             s->rz = tot[2];
+            s->rr_cap = INFINITY;
             s->iterations = 0;
             s->status = 0;
             s->done = 0;
@@ -739,6 +743,9 @@ __global__ void __launch_bounds__(kRedThreads) k_true_residual(
             s->abs_new = tot[1];
             s->rz = tot[1];
             s->rr = tot[0];
+            // a cycle whose FP32 recurrence r.r grows to this multiple of the replaced one has
+            // diverged (CG residual norms are not monotone: a factor 1000 in the norm)
+            s->rr_cap = 1e6 * tot[0];
             s->counter[3] = 0;
         }
     }
@@ -783,11 +790,17 @@ int pcg_reliable_mixed(nb2_ctx* c, const double* b, double* x, double tol, doubl
     *iterations = 0;
     if (b2 == 0.0) return NB2_OK;
     double* rr_dev = c->norms + 6;
+    int resets = 0;
     for (int update = 0;; ++update) {
         if (!c->h_cgs->done) NB2_TRY(cg.run(maxit));
         const CgScalars h = *c->h_cgs;
         *iterations = h.iterations;
-        if (h.status && h.status != NB2_E_CG_MAXIT) return h.status;
+        // a diverged cycle (its kept search direction no longer fits the replaced residual,
+        // near the FP32 operator's accuracy floor): replace the residual again and restart the
+        // cycle with p = D^-1 r, at most three times per solve
+        const bool fresh = h.status == NB2_E_CG_BREAKDOWN && resets < 3;
+        if (fresh) ++resets;
+        if (h.status && h.status != NB2_E_CG_MAXIT && !fresh) return h.status;
         // reliable update: x += xs; r = b - K x in FP64
         k_fold<<<grid, 256, 0, c->stream>>>(n, cg.x, x);
         NB2_TRY(launch_apply(c, x, work));
@@ -817,6 +830,11 @@ int pcg_reliable_mixed(nb2_ctx* c, const double* b, double* x, double tol, doubl
                                     c->stream));
         NB2_CUDA(c, cudaMemcpyAsync(&c->cgs->status, &upd.status, sizeof(int),
                                     cudaMemcpyHostToDevice, c->stream));
+        if (fresh) {
+            static const double zero = 0.0;
+            NB2_CUDA(c, cudaMemcpyAsync(&c->cgs->beta, &zero, sizeof(double),
+                                        cudaMemcpyHostToDevice, c->stream));
+        }
         k_p<float><<<cg.RB, kRedThreads, 0, c->stream>>>(n, cg.p, cg.r, cg.inv, c->cgs);
         c->launches++;
         NB2_TRY(wait_scalars(c));
