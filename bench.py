@@ -72,17 +72,60 @@ def plastic_displacement(mesh, level=2.5e-3):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clocks and clock-event reasons during the timed region, read (never set) through NVML
+    from a thread polling every 5 ms, with one sample at start and one at stop, so that even a
+    timed region of a few tens of milliseconds has samples; `nvidia-smi -lms 200` as the
+    fallback when NVML is not importable."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("sw_power_cap", 0x4), ("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20),
+               ("hw_thermal_slowdown", 0x40))
 
     def __init__(self, index=0):
         self.index = index
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm MHz, max sm MHz, reasons bitmask)
+        self.stop_event = threading.Event()
+
+    def _nvml_sample(self):
+        nv, h = self.nvml
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h) \
+                if hasattr(nv, "nvmlDeviceGetCurrentClocksEventReasons") \
+                else nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            self.samples.append((float(sm), float(smax), int(reasons)))
+        except Exception:  # a failed read leaves a gap, not an error
+            pass
+
+    def _poll(self):
+        while not self.stop_event.wait(0.005):
+            self._nvml_sample()
 
     def start(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            bus = None
+            try:
+                import torch
+                pr = torch.cuda.get_device_properties(torch.cuda.current_device())
+                bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            except Exception:
+                bus = None
+            h = nv.nvmlDeviceGetHandleByPciBusId(bus) if bus else \
+                nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.nvml = (nv, h)
+            self._nvml_sample()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
@@ -98,6 +141,20 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_event.set()
+            self.thread.join(timeout=5)
+            self._nvml_sample()
+            sm = [x[0] for x in self.samples]
+            smax = max((x[1] for x in self.samples), default=None)
+            reasons = sorted({name for _, _, m in self.samples for name, bit in self.REASONS
+                              if m & bit})
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -120,7 +177,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def algorithmic_work(mesh_size, nnz, n_nodes, E, nqp, fp64=True):
