@@ -47,7 +47,7 @@ typedef enum nb2_model {
     NB2_ISOTROPIC_LINEAR_ELASTICITY = 0, /* "isotropic_linear_elasticity" */
     NB2_NEOHOOKE = 1,                    /* "neohooke" */
     NB2_SMALL_STRAIN_J2_PLASTICITY = 2,  /* "J2_plasticity", "finite_strain": false */
-    NB2_GAUSSIAN_AFFINE_MICROSPHERE = 3, /* "microsphere", "affine", "gaussian", "BO21" */
+    NB2_GAUSSIAN_AFFINE_MICROSPHERE = 3, /* "microsphere", "affine", "gaussian", "BO21"/"BO33" */
     NB2_LANGEVIN_AFFINE_MICROSPHERE = 4, /* "microsphere", "affine", "langevin", "BO21"
                                             (affine_microsphere.cpp:23-112) */
     NB2_NONAFFINE_MICROSPHERE = 5        /* "microsphere", "nonaffine", "BO21"
@@ -89,6 +89,8 @@ typedef struct nb2_material {
     double isotropic_hardening_modulus;
     double segments_per_chain;
     double nonaffine_stretch_parameter;
+    int32_t unit_sphere_points; /* microsphere models: 21 (BO21; also when 0) or 33 (BO33),
+                                   unit_sphere_quadrature.cpp:10-91 */
 } nb2_material;
 
 /* A time/value table applied to a DOF list: a Dirichlet boundary (mesh/boundary/nodal_value.cpp,

@@ -53,7 +53,8 @@ class MaterialDesc(C.Structure):
                 ("shear_modulus", C.c_double), ("yield_stress", C.c_double),
                 ("isotropic_hardening_modulus", C.c_double),
                 ("segments_per_chain", C.c_double),
-                ("nonaffine_stretch_parameter", C.c_double)]
+                ("nonaffine_stretch_parameter", C.c_double),
+                ("unit_sphere_points", C.c_int32)]
 
 
 class DofTableDesc(C.Structure):
@@ -176,7 +177,7 @@ class SolidMesh:
                         self.conn.shape[1], self.conn.ctypes.data)
         mat = MaterialDesc(int(material.model), material.K, material.G, material.yield_stress,
                            material.hardening, material.segments_per_chain,
-                           material.nonaffine_stretch_parameter)
+                           material.nonaffine_stretch_parameter, material.unit_sphere_points)
         h = P()
         _check(L.nb2_create(C.byref(desc), C.byref(mat), C.byref(h)), None, "nb2_create")
         self.h = h

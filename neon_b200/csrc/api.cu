@@ -148,7 +148,9 @@ int nb2_create(const nb2_mesh_desc* m, const nb2_material* mat, nb2_ctx** out) {
     *out = nullptr;
     if (!m || !mat || !m->coordinates || !m->connectivity || m->num_nodes <= 0 ||
         m->num_elements <= 0 || (m->nodes_per_element != 8 && m->nodes_per_element != 4) ||
-        mat->model < 0 || mat->model > 5) {
+        mat->model < 0 || mat->model > 5 ||
+        (mat->unit_sphere_points != 0 && mat->unit_sphere_points != 21 &&
+         mat->unit_sphere_points != 33)) {
         g_create_error = "invalid mesh or material description";
         return NB2_E_INPUT;
     }

@@ -45,8 +45,9 @@ __constant__ double c_w_hex8[8];
 __constant__ double c_dN_tet4[4 * 3];
 __constant__ float c_dNf_hex8[8 * 8 * 3];  // FP32 copies for the matrix-free FP32 operator
 __constant__ float c_dNf_tet4[4 * 3];
-__constant__ double c_sphere_r[21 * 3];
-__constant__ double c_sphere_w[21];
+// unit-sphere rules of the microsphere models, side by side: BO21 at 0, BO33 at 21
+__constant__ double c_sphere_r[(21 + 33) * 3];
+__constant__ double c_sphere_w[21 + 33];
 
 // (row, first column, count) of the upper-triangular blocks owned by each lane of a group
 __constant__ int c_seg_hex8[8][6] = {{0, 0, 5, 0, 0, 0}, {0, 5, 3, 7, 7, 1}, {1, 1, 5, 0, 0, 0},
@@ -221,7 +222,7 @@ __device__ __forceinline__ void cm_microsphere(const ElementArgs& A, double Gm, 
     for (int i = 0; i < 9; ++i) Fb[i] = sc * F[i];
     double acc[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll 3
-    for (int i = 0; i < 21; ++i) {
+    for (int i = A.sph0; i < A.sph0 + A.nsph; ++i) {
         double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1], r2 = c_sphere_r[3 * i + 2];
         double w = c_sphere_w[i];
         double t0 = Fb[0] * r0 + Fb[1] * r1 + Fb[2] * r2;
@@ -272,7 +273,7 @@ __device__ __forceinline__ void cm_langevin(const ElementArgs& A, double Gm, con
 #pragma unroll
     for (int c = 0; c < 21; ++c) o.Da[c] = 0.0;
 #pragma unroll 1
-    for (int i = 0; i < 21; ++i) {
+    for (int i = A.sph0; i < A.sph0 + A.nsph; ++i) {
         double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1], r2 = c_sphere_r[3 * i + 2];
         double w = c_sphere_w[i];
         double t0 = Fb[0] * r0 + Fb[1] * r1 + Fb[2] * r2;
@@ -358,7 +359,7 @@ __device__ __forceinline__ void cm_nonaffine(const ElementArgs& A, double Gm, co
 #pragma unroll
     for (int c = 0; c < 21; ++c) H[c] = C[c] = 0.0;
 #pragma unroll 1
-    for (int i = 0; i < 21; ++i) {
+    for (int i = A.sph0; i < A.sph0 + A.nsph; ++i) {
         const double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1], r2 = c_sphere_r[3 * i + 2];
         const double w = c_sphere_w[i];
         const double t[3] = {Fb[0] * r0 + Fb[1] * r1 + Fb[2] * r2,
@@ -722,7 +723,7 @@ __global__ void __launch_bounds__(64) k_adjoint_shear(ElementArgs A, const doubl
         const double sc = pow(J, -1.0 / 3.0);
         double acc[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll 3
-        for (int i = 0; i < 21; ++i) {
+        for (int i = A.sph0; i < A.sph0 + A.nsph; ++i) {
             const double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1],
                          r2 = c_sphere_r[3 * i + 2], wi = c_sphere_w[i];
             const double t0 = sc * (Fd[0] * r0 + Fd[1] * r1 + Fd[2] * r2);
@@ -842,7 +843,7 @@ __device__ __forceinline__ void dual_stress(const ElementArgs& A, double Gm, con
         const Dual J = ddet3(F);
         const Dual sc = dpow(J, -1.0 / 3.0);
         Dual acc[6] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}};
-        for (int i = 0; i < 21; ++i) {
+        for (int i = A.sph0; i < A.sph0 + A.nsph; ++i) {
             const double r0 = c_sphere_r[3 * i], r1 = c_sphere_r[3 * i + 1],
                          r2 = c_sphere_r[3 * i + 2], w = c_sphere_w[i];
             const Dual t0 = sc * (r0 * F[0] + r1 * F[1] + r2 * F[2]);
@@ -1010,12 +1011,28 @@ static int upload_tables(nb2_ctx* c) {
                               0, d0, d0, 0, d0, -d0, d1, d1, d2, d1, d1, -d2, d1, -d1, d2, d1, -d1,
                               -d2, d1, d2, d1, d1, d2, -d1, d1, -d2, d1, d1, -d2, -d1, d2, d1, d1,
                               d2, d1, -d1, d2, -d1, d1, d2, -d1, -d1};
-    double sw[21];
+    // BO33 (unit_sphere_quadrature.cpp:33-91), after BO21 in the same tables
+    const double v1 = 2.0 * 0.00985353993433, v2 = 2.0 * 0.0162969685886,
+                 v3 = 2.0 * 0.0134788844008, v4 = 2.0 * 0.0175759129880;
+    const double a = 0.707106781187, b = 0.933898956394, cc = 0.357537045978,
+                 d = 0.437263676092, ee = 0.785875915868;
+    const double r33[33 * 3] = {1, 0, 0, 0, 1, 0, 0, 0, 1,
+                                a, a, 0, a, -a, 0, a, 0, a, a, 0, -a, 0, a, a, 0, a, -a,
+                                b, cc, 0, b, -cc, 0, cc, b, 0, cc, -b, 0,
+                                b, 0, cc, b, 0, -cc, cc, 0, b, cc, 0, -b,
+                                0, b, cc, 0, b, -cc, 0, cc, b, 0, cc, -b,
+                                d, d, ee, d, d, -ee, d, -d, ee, d, -d, -ee,
+                                d, ee, d, d, ee, -d, d, -ee, d, d, -ee, -d,
+                                ee, d, d, ee, d, -d, ee, -d, d, ee, -d, -d};
+    double rr[(21 + 33) * 3], sw[21 + 33];
+    for (int i = 0; i < 21 * 3; ++i) rr[i] = r[i];
+    for (int i = 0; i < 33 * 3; ++i) rr[21 * 3 + i] = r33[i];
     for (int i = 0; i < 21; ++i) sw[i] = i < 3 ? w1 : (i < 9 ? w2 : w3);
+    for (int i = 0; i < 33; ++i) sw[21 + i] = i < 3 ? v1 : (i < 9 ? v2 : (i < 21 ? v3 : v4));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_dN_hex8, dN, sizeof dN));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_w_hex8, w, sizeof w));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_dN_tet4, dNt, sizeof dNt));
-    NB2_CUDA(c, cudaMemcpyToSymbol(c_sphere_r, r, sizeof r));
+    NB2_CUDA(c, cudaMemcpyToSymbol(c_sphere_r, rr, sizeof rr));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_sphere_w, sw, sizeof sw));
     float dNf[8 * 8 * 3], dNtf[12];
     for (int i = 0; i < 8 * 8 * 3; ++i) dNf[i] = (float)dN[i];
@@ -1216,6 +1233,8 @@ static ElementArgs make_args(nb2_ctx* c) {
     A.H_iso = c->mat.isotropic_hardening_modulus;
     A.Nseg = c->mat.segments_per_chain;
     A.p_na = c->mat.nonaffine_stretch_parameter;
+    A.sph0 = c->mat.unit_sphere_points == 33 ? 21 : 0;
+    A.nsph = c->mat.unit_sphere_points == 33 ? 33 : 21;
     A.Ge = c->Ge;
     A.Ke = c->Ke;
     A.ep = c->ep;

@@ -68,6 +68,7 @@ struct ElementArgs {
     double K, G, lambda, sigma_y, H_iso;
     double Nseg;       // segments per chain (Langevin and non-affine microsphere)
     double p_na;       // non-affine stretch parameter
+    int sph0, nsph;    // unit-sphere rule of the microsphere models: first point, count
     const double* Ge;  // per-element shear modulus (or null)
     const double* Ke;  // per-element bulk modulus (or null)
     double* ep;      // [6][nqp]

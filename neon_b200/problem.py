@@ -41,6 +41,7 @@ class Material:
     hardening: float = 0.0
     segments_per_chain: float = 0.0
     nonaffine_stretch_parameter: float = 0.0
+    unit_sphere_points: int = 21  # microsphere quadrature: BO21 or BO33
 
     @property
     def lam(self) -> float:
@@ -48,8 +49,8 @@ class Material:
 
     def params(self) -> np.ndarray:
         return np.array([self.K, self.G, self.yield_stress, self.hardening,
-                         self.segments_per_chain, self.nonaffine_stretch_parameter],
-                        dtype=np.float64)
+                         self.segments_per_chain, self.nonaffine_stretch_parameter,
+                         float(self.unit_sphere_points)], dtype=np.float64)
 
 
 def _check_microsphere_options(constitutive: dict):
@@ -108,10 +109,11 @@ def make_material(material: dict, constitutive: dict) -> Material:
                         float(material.get("isotropic_hardening_modulus", 0.0)))
     if name == "microsphere":
         affine = constitutive["type"] == "affine"
-        if constitutive["quadrature"] != "BO21" or \
+        if constitutive["quadrature"] == "FM900" or \
                 (affine and "ageing" in constitutive and constitutive["statistics"] == "gaussian"):
-            raise NotImplementedError("only the BO21 microsphere models (affine Gaussian, affine "
-                                      "Langevin, non-affine) are on this path")
+            raise NotImplementedError("the microsphere models (affine Gaussian, affine Langevin, "
+                                      "non-affine) are on this path with the BO21 and BO33 rules")
+        points = 33 if constitutive["quadrature"] == "BO33" else 21
         if "segments_per_chain" not in material:
             raise ValueError("segments_per_chain not specified in material data")
         N = float(material["segments_per_chain"])
@@ -120,10 +122,11 @@ def make_material(material: dict, constitutive: dict) -> Material:
                 raise ValueError('"nonaffine_stretch_parameter" not specified in material data')
             return Material(NONAFFINE_MICROSPHERE, K, G, segments_per_chain=N,
                             nonaffine_stretch_parameter=float(
-                                material["nonaffine_stretch_parameter"]))
+                                material["nonaffine_stretch_parameter"]),
+                            unit_sphere_points=points)
         model = GAUSS_AFFINE_MICROSPHERE if constitutive["statistics"] == "gaussian" \
             else LANGEVIN_AFFINE_MICROSPHERE
-        return Material(model, K, G, segments_per_chain=N)
+        return Material(model, K, G, segments_per_chain=N, unit_sphere_points=points)
     raise ValueError(f"The model name {name} is not recognised")
 
 

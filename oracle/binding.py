@@ -71,7 +71,8 @@ def lib():
         L.orc_cg_sample.restype = C.c_double
         L.orc_cg_sample.argtypes = [C.c_int, ip, ip, dp, dp, C.c_int, C.c_int,
                                     C.POINTER(C.c_double)]
-        L.orc_sphere_rule.argtypes = [dp, dp]
+        L.orc_sphere_rule.argtypes = [C.c_int, dp, dp]
+        L.orc_sphere_rule.restype = C.c_int
         L.orc_shape.argtypes = [C.c_int, dp, dp]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_max_threads.restype = C.c_int
@@ -101,11 +102,12 @@ class OrcReport(C.Structure):
                 ("seconds_solve", C.c_double), ("message", C.c_char * 256)]
 
 
-def sphere_rule():
-    r = np.zeros(63)
-    w = np.zeros(21)
-    lib().orc_sphere_rule(r, w)
-    return r.reshape(21, 3), w
+def sphere_rule(points: int = 21):
+    """Directions [n][3] and weights [n] of the BO21 (points=21) or BO33 (points=33) rule."""
+    r = np.zeros(33 * 3)
+    w = np.zeros(33)
+    n = lib().orc_sphere_rule(int(points), r, w)
+    return r[:3 * n].reshape(n, 3), w[:n]
 
 
 def shape(npe: int):

@@ -229,10 +229,12 @@ Interpolation make_tet4() {
     return I;
 }
 
-// BO21 unit-sphere rule (quadrature/sphere/unit_sphere_quadrature.cpp:10-31)
+// Unit-sphere rules of the microsphere models (quadrature/sphere/unit_sphere_quadrature.cpp):
+// BO21 (:10-31) and BO33 (:33-91), both from Bazant and Oh (1986), Table 1
 struct SphereRule {
-    double r[21][3];
-    double w[21];
+    int n = 0;
+    double r[33][3];
+    double w[33];
 };
 
 SphereRule make_bo21() {
@@ -246,9 +248,33 @@ SphereRule make_bo21() {
                                {dc1, -dc1, -dc2}, {dc1, dc2, dc1},    {dc1, dc2, -dc1},
                                {dc1, -dc2, dc1},  {dc1, -dc2, -dc1},  {dc2, dc1, dc1},
                                {dc2, dc1, -dc1},  {dc2, -dc1, dc1},   {dc2, -dc1, -dc1}};
+    s.n = 21;
     for (int i = 0; i < 21; ++i) {
         for (int k = 0; k < 3; ++k) s.r[i][k] = pts[i][k];
         s.w[i] = (i < 3) ? w1 : (i < 9 ? w2 : w3);
+    }
+    return s;
+}
+
+SphereRule make_bo33() {
+    SphereRule s;
+    const double w1 = 2.0 * 0.00985353993433, w2 = 2.0 * 0.0162969685886,
+                 w3 = 2.0 * 0.0134788844008, w4 = 2.0 * 0.0175759129880;
+    const double a = 0.707106781187, b = 0.933898956394, c = 0.357537045978, d = 0.437263676092,
+                 e = 0.785875915868;
+    const double pts[33][3] = {
+        {1, 0, 0},  {0, 1, 0},   {0, 0, 1},                                         // 3 axes
+        {a, a, 0},  {a, -a, 0},  {a, 0, a},  {a, 0, -a},  {0, a, a},  {0, a, -a},   // 6 edges
+        {b, c, 0},  {b, -c, 0},  {c, b, 0},  {c, -b, 0},                            // 12 (b, c)
+        {b, 0, c},  {b, 0, -c},  {c, 0, b},  {c, 0, -b},
+        {0, b, c},  {0, b, -c},  {0, c, b},  {0, c, -b},
+        {d, d, e},  {d, d, -e},  {d, -d, e}, {d, -d, -e},                           // 12 (d, e)
+        {d, e, d},  {d, e, -d},  {d, -e, d}, {d, -e, -d},
+        {e, d, d},  {e, d, -d},  {e, -d, d}, {e, -d, -d}};
+    s.n = 33;
+    for (int i = 0; i < 33; ++i) {
+        for (int k = 0; k < 3; ++k) s.r[i][k] = pts[i][k];
+        s.w[i] = i < 3 ? w1 : (i < 9 ? w2 : (i < 21 ? w3 : w4));
     }
     return s;
 }
@@ -262,6 +288,7 @@ struct Material {
     double sigma_y = 0, H_iso = 0;   // isotropic_elastic_plastic.cpp:10-38
     double segments = 0;             // micromechanical_elastomer.cpp:13-21
     double nonaffine_p = 0;          // nonaffine_microsphere.cpp:17-25
+    int sphere_points = 21;          // unit-sphere rule of the microsphere models (BO21 / BO33)
     double lambda() const { return K - 2.0 * G / 3.0; }  // isotropic_elastic_property.hpp:28
 };
 
@@ -446,7 +473,7 @@ void update_microsphere(Oracle& o, size_t q, double G, bool langevin = false) {
     // G sum_i w_i pade_first t_i (x) t_i (Langevin); compute_macro_moduli (Langevin)
     double acc[9] = {0};
     double macroC[36] = {0};
-    for (int i = 0; i < 21; ++i) {
+    for (int i = 0; i < o.sphere.n; ++i) {
         double t[3];
         for (int a = 0; a < 3; ++a)
             t[a] = Fb[a * 3 + 0] * o.sphere.r[i][0] + Fb[a * 3 + 1] * o.sphere.r[i][1] +
@@ -559,7 +586,7 @@ void update_nonaffine(Oracle& o, size_t q, double G) {
     for (int i = 0; i < 9; ++i) Fb[i] = scale * Fq[i];
     inv3(Fb, Fbi);
     double lp = 0.0, h[9] = {0}, H[36] = {0}, k[9] = {0}, KG[36] = {0};
-    for (int i = 0; i < 21; ++i) {
+    for (int i = 0; i < o.sphere.n; ++i) {
         const double* r = o.sphere.r[i];
         const double w = o.sphere.w[i];
         double t[3], n[3];
@@ -1393,6 +1420,8 @@ void* orc_create(int num_nodes, const double* coords, int num_elements, int node
     o->mat.H_iso = params[3];
     o->mat.segments = params[4];
     o->mat.nonaffine_p = params[5];
+    o->mat.sphere_points = params[6] == 33.0 ? 33 : 21;
+    o->sphere = o->mat.sphere_points == 33 ? make_bo33() : make_bo21();
     if (Ge) o->Ge.assign(Ge, Ge + num_elements);
     size_t nqp = (size_t)num_elements * o->nq;
     o->H.assign(nqp * 9, 0.0);
@@ -1413,13 +1442,14 @@ void* orc_create(int num_nodes, const double* coords, int num_elements, int node
 
 void orc_destroy(void* h) { delete static_cast<Oracle*>(h); }
 
-// BO21 directions [21][3] and weights [21] (unit_sphere_quadrature.cpp:10-31)
-void orc_sphere_rule(double* r, double* w) {
-    SphereRule s = make_bo21();
-    for (int i = 0; i < 21; ++i) {
+// directions [n][3] and weights [n] of the BO21 (points 21) or BO33 (points 33) rule; returns n
+int orc_sphere_rule(int points, double* r, double* w) {
+    SphereRule s = points == 33 ? make_bo33() : make_bo21();
+    for (int i = 0; i < s.n; ++i) {
         for (int k = 0; k < 3; ++k) r[3 * i + k] = s.r[i][k];
         w[i] = s.w[i];
     }
+    return s.n;
 }
 
 // hex8 (npe 8) or tet4 (npe 4) shape derivatives [nq][npe][3] and weights [nq]

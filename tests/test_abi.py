@@ -44,7 +44,7 @@ def test_create_rejects_bad_input_without_gpu():
     X = np.zeros((4, 3))
     conn = np.array([[0, 1, 2, 7]], np.int32)  # node 7 does not exist
     desc = api.MeshDesc(4, X.ctypes.data, 1, 4, conn.ctypes.data)
-    mat = api.MaterialDesc(0, 1.0, 1.0, 0, 0, 0, 0)
+    mat = api.MaterialDesc(0, 1.0, 1.0, 0, 0, 0, 0, 0)
     h = ctypes.c_void_p()
     assert L.nb2_create(ctypes.byref(desc), ctypes.byref(mat), ctypes.byref(h)) == api.E_INPUT
     buf = ctypes.create_string_buffer(256)
@@ -85,9 +85,11 @@ def test_microsphere_factory_errors():
         m = P.make_material(rubber, {**ms, "type": "affine", "quadrature": "BO21",
                                      "statistics": statistics})
         assert m.model == model and m.segments_per_chain == 50
-    with pytest.raises(NotImplementedError):  # other quadrature rules
+    with pytest.raises(NotImplementedError):  # the 900-point rule is not on this path
         P.make_material(rubber, {**ms, "type": "affine", "quadrature": "FM900",
                                  "statistics": "langevin"})
+    assert P.make_material(rubber, {**ms, "type": "affine", "quadrature": "BO33",
+                                    "statistics": "langevin"}).unit_sphere_points == 33
     # test/hyperelastic_constitutive.cpp "Nonaffine microsphere" exception: a misspelt
     # nonaffine_stretch_parameter
     with pytest.raises(ValueError):

@@ -46,12 +46,22 @@ MATERIALS = {
                                   "segments_per_chain": 5, "nonaffine_stretch_parameter": 1.5},
                                  {"name": "microsphere", "type": "nonaffine",
                                   "quadrature": "BO21"}),
+    # the 33-point unit-sphere rule on the affine and on the anisotropic tangent path
+    "microsphere_bo33": P.make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0,
+                                         "segments_per_chain": 50},
+                                        {"name": "microsphere", "type": "affine",
+                                         "statistics": "gaussian", "quadrature": "BO33"}),
+    "nonaffine_bo33": P.make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0,
+                                       "segments_per_chain": 5,
+                                       "nonaffine_stretch_parameter": 1.5},
+                                      {"name": "microsphere", "type": "nonaffine",
+                                       "quadrature": "BO33"}),
 }
 # displacement amplitudes that keep det F > 0 and put J2 points in the plastic range
 SCALE = {"linear_elastic": 1e-3, "neohooke": 0.02, "j2": 4e-3, "microsphere": 0.02,
-         "langevin": 0.03, "nonaffine": 0.03}
+         "langevin": 0.03, "nonaffine": 0.03, "microsphere_bo33": 0.02, "nonaffine_bo33": 0.03}
 # models with a per-element shear modulus field in the tests
-FIELD_MODELS = ("microsphere", "langevin", "nonaffine")
+FIELD_MODELS = ("microsphere", "langevin", "nonaffine", "microsphere_bo33", "nonaffine_bo33")
 
 
 def _meshes():

@@ -267,6 +267,33 @@ def test_quadrature_rules(oracle, kats):
     assert vol == pytest.approx(k["unit_cube_volume"])
 
 
+def test_bo33_unit_sphere_rule(oracle):
+    """The 33-point rule (Bazant and Oh 1986, unit_sphere_quadrature.cpp:33-91): unit directions,
+    weights summing to 1, isotropic second moment, and the microsphere models on it stress-free
+    at F = I and close to the 21-point rule under stretch (both integrate the same sphere)."""
+    r, w = oracle.sphere_rule(33)
+    assert len(w) == 33 and w.sum() == pytest.approx(1.0, abs=1e-11)
+    np.testing.assert_allclose(np.linalg.norm(r, axis=1), 1.0, rtol=1e-11)
+    np.testing.assert_allclose((w[:, None, None] * r[:, :, None] * r[:, None, :]).sum(0),
+                               np.eye(3) / 3.0, atol=1e-11)
+    sig = {}
+    for q in ("BO21", "BO33"):
+        mat = P.make_material({"bulk_modulus": 100.0, "shear_modulus": 1.0,
+                               "segments_per_chain": 8},
+                              {"name": "microsphere", "type": "affine", "statistics": "langevin",
+                               "quadrature": q})
+        assert mat.unit_sphere_points == int(q[2:])
+        om = _single_point(oracle, mat)
+        om.set("F", np.tile(np.eye(3).reshape(-1), (2, 1)))
+        om.set("detF", np.ones(2))
+        om.constitutive_only()
+        assert np.abs(om.get("sigma")).max() < 1e-5
+        assert all(_is_spd(D) for D in om.get("D"))
+        _uniaxial(om, 1.3)
+        sig[q] = om.get("sigma")[0].reshape(3, 3)
+    assert np.abs(sig["BO33"] - sig["BO21"]).max() < 0.02 * np.abs(sig["BO21"]).max()
+
+
 def test_cube_fixture_element_symmetry(oracle, kats):
     k = kats["cube_fixture"]
     m = M.structured_hex8(3)
