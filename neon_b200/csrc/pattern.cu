@@ -88,6 +88,13 @@ int build_pattern(nb2_ctx* c) {
     thrust::sort(pol, kp, kp + pairs);
     auto end = thrust::unique(pol, kp, kp + pairs);
     long long m = end - kp;
+    if (9 * m > 2147483647ll) {
+        // the CSR export (and neon's Eigen matrix) index entries with int32
+        cudaFreeAsync(keys, c->stream);
+        c->error = "the stiffness pattern has more than 2^31 - 1 entries: beyond the int32 row "
+                   "pointers and column indices of the CSR matrix";
+        return NB2_E_INPUT;
+    }
     c->nnzb = m;
     c->nnz = 9 * m;
     int* count = nullptr;
