@@ -644,8 +644,9 @@ extern "C" int nb2_adjoint_shear_gradient(nb2_ctx* c, const double* dJdu, int32_
                                           double tol, int32_t maxit, double* dJdG,
                                           int32_t* iterations) {
     if (!c || !dJdu || !dJdG || maxit <= 0) return NB2_E_INPUT;
-    if (c->mat.model != NB2_GAUSSIAN_AFFINE_MICROSPHERE) {
-        c->error = "the shear-modulus adjoint is defined for the Gaussian affine microsphere";
+    if (c->mat.model != NB2_GAUSSIAN_AFFINE_MICROSPHERE &&
+        c->mat.model != NB2_LANGEVIN_AFFINE_MICROSPHERE) {
+        c->error = "the shear-modulus adjoint is defined for the affine microsphere models";
         return NB2_E_INPUT;
     }
     if (!c->Ge) {  // uniform field = the material modulus

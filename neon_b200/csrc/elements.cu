@@ -663,15 +663,16 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
 #include "mf_kernels.cuh"
 
 // ---------------------------------------------------------------------------------------
-// Adjoint gradient with respect to the per-element shear modulus of the Gaussian affine
-// microsphere.  With K lambda = dJ/du solved on the converged tangent,
+// Adjoint gradient with respect to the per-element shear modulus of the Gaussian or Langevin
+// affine microsphere.  With K lambda = dJ/du solved on the converged tangent,
 //   dJ/dG_e = - lambda^T df_int/dG_e = - sum_q s_q (d sigma_q / dG) : grad(lambda)_q,
-// where sigma = (p I + dev tau)/J and tau = 3 G sum_i w_i t_i (x) t_i (t_i = Fbar r_i), so
-// d sigma/dG = dev(3 sum_i w_i t_i (x) t_i) / J.  The quadrature-point state (F, Fbar, the
+// where sigma = (p I + dev tau)/J and tau = G sum_i w_i f_i t_i (x) t_i (t_i = Fbar r_i; chain
+// weight f_i = 3 Gaussian, pade_first(|t_i|, N) Langevin), so
+// d sigma/dG = dev(sum_i w_i f_i t_i (x) t_i) / J.  The quadrature-point state (F, Fbar, the
 // sphere sum) is recomputed from the displacement, not stored.  One value per element: the
 // group reduces over its points with shuffles, no atomics.
 // ---------------------------------------------------------------------------------------
-template <int NPE>
+template <int NPE, int MODEL>
 __global__ void __launch_bounds__(64) k_adjoint_shear(ElementArgs A, const double* __restrict__ lam,
                                                       double* __restrict__ dJdG) {
     using T = Topo<NPE>;
@@ -729,18 +730,23 @@ __global__ void __launch_bounds__(64) k_adjoint_shear(ElementArgs A, const doubl
             const double t0 = sc * (Fd[0] * r0 + Fd[1] * r1 + Fd[2] * r2);
             const double t1 = sc * (Fd[3] * r0 + Fd[4] * r1 + Fd[5] * r2);
             const double t2 = sc * (Fd[6] * r0 + Fd[7] * r1 + Fd[8] * r2);
-            acc[0] += (t0 * t0) * wi;
-            acc[1] += (t1 * t1) * wi;
-            acc[2] += (t2 * t2) * wi;
-            acc[3] += (t1 * t2) * wi;
-            acc[4] += (t0 * t2) * wi;
-            acc[5] += (t0 * t1) * wi;
+            double f = 3.0;
+            if constexpr (MODEL == MODEL_ML) {
+                const double l2 = t0 * t0 + t1 * t1 + t2 * t2;
+                f = (3.0 * A.Nseg - l2) / (A.Nseg - l2);
+            }
+            const double wf = wi * f;
+            acc[0] += (t0 * t0) * wf;
+            acc[1] += (t1 * t1) * wf;
+            acc[2] += (t2 * t2) * wf;
+            acc[3] += (t1 * t2) * wf;
+            acc[4] += (t0 * t2) * wf;
+            acc[5] += (t0 * t1) * wf;
         }
-        // d sigma / dG = dev(3 acc) / J  (11 22 33 23 13 12)
-        const double tr3 = (acc[0] + acc[1] + acc[2]);  // (3 acc) trace / 3
-        double ds[6] = {(3.0 * acc[0] - tr3) / J, (3.0 * acc[1] - tr3) / J,
-                        (3.0 * acc[2] - tr3) / J, 3.0 * acc[3] / J,
-                        3.0 * acc[4] / J,         3.0 * acc[5] / J};
+        // d sigma / dG = dev(acc) / J  (11 22 33 23 13 12)
+        const double tr3 = (acc[0] + acc[1] + acc[2]) / 3.0;
+        double ds[6] = {(acc[0] - tr3) / J, (acc[1] - tr3) / J, (acc[2] - tr3) / J,
+                        acc[3] / J,         acc[4] / J,         acc[5] / J};
         inv3(Fc, Ji);
         const double s = w * det3(Fc);
         double Gm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -849,16 +855,24 @@ __device__ __forceinline__ void dual_stress(const ElementArgs& A, double Gm, con
             const Dual t0 = sc * (r0 * F[0] + r1 * F[1] + r2 * F[2]);
             const Dual t1 = sc * (r0 * F[3] + r1 * F[4] + r2 * F[5]);
             const Dual t2 = sc * (r0 * F[6] + r1 * F[7] + r2 * F[8]);
-            acc[0] = acc[0] + w * (t0 * t0);
-            acc[1] = acc[1] + w * (t1 * t1);
-            acc[2] = acc[2] + w * (t2 * t2);
-            acc[3] = acc[3] + w * (t1 * t2);
-            acc[4] = acc[4] + w * (t0 * t2);
-            acc[5] = acc[5] + w * (t0 * t1);
+            // chain weight: 3 (Gaussian) or the Pade approximant pade_first(l) (Langevin)
+            Dual f{3.0, 0.0};
+            if constexpr (MODEL == MODEL_ML) {
+                const Dual l2 = t0 * t0 + t1 * t1 + t2 * t2;
+                const Dual Nd{A.Nseg, 0.0};
+                f = (3.0 * Nd - l2) / (Nd - l2);
+            }
+            const Dual wf = w * f;
+            acc[0] = acc[0] + wf * (t0 * t0);
+            acc[1] = acc[1] + wf * (t1 * t1);
+            acc[2] = acc[2] + wf * (t2 * t2);
+            acc[3] = acc[3] + wf * (t1 * t2);
+            acc[4] = acc[4] + wf * (t0 * t2);
+            acc[5] = acc[5] + wf * (t0 * t1);
         }
         Dual tau[6];
 #pragma unroll
-        for (int c = 0; c < 6; ++c) tau[c] = (3.0 * Gm) * acc[c];
+        for (int c = 0; c < 6; ++c) tau[c] = Gm * acc[c];
         const Dual invJ = Dual{1.0, 0.0} / J;
         const Dual p = J * ((K / 2.0) * (J - invJ));
         const Dual tr3 = (1.0 / 3.0) * (tau[0] + tau[1] + tau[2]);
@@ -1184,7 +1198,8 @@ static int launch_jvp_t(nb2_ctx* c, const ElementArgs& A, const double* v, doubl
         case MODEL_LE: k_force_jvp<NPE, MODEL_LE><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         case MODEL_NH: k_force_jvp<NPE, MODEL_NH><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         case MODEL_MS: k_force_jvp<NPE, MODEL_MS><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
-        default: return NB2_E_INPUT;  // J2 carries history; no Langevin product here
+        case MODEL_ML: k_force_jvp<NPE, MODEL_ML><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
+        default: return NB2_E_INPUT;  // J2 carries history; the non-affine model has no product here
     }
     c->launches++;
     return NB2_OK;
@@ -1206,12 +1221,21 @@ int launch_adjoint_shear(nb2_ctx* c, const double* lam, double* dJdG) {
     int st = upload_tables(c);
     if (st) return st;
     ElementArgs A = make_args(c);
+    const bool lgv = c->mat.model == MODEL_ML;
     if (c->npe == 8) {
         constexpr int EPC = Topo<8>::EPC, G = Topo<8>::G;
-        k_adjoint_shear<8><<<(c->E + EPC - 1) / EPC, EPC * G, 0, c->stream>>>(A, lam, dJdG);
+        const unsigned grid = (unsigned)((c->E + EPC - 1) / EPC);
+        if (lgv)
+            k_adjoint_shear<8, MODEL_ML><<<grid, EPC * G, 0, c->stream>>>(A, lam, dJdG);
+        else
+            k_adjoint_shear<8, MODEL_MS><<<grid, EPC * G, 0, c->stream>>>(A, lam, dJdG);
     } else {
         constexpr int EPC = Topo<4>::EPC, G = Topo<4>::G;
-        k_adjoint_shear<4><<<(c->E + EPC - 1) / EPC, EPC * G, 0, c->stream>>>(A, lam, dJdG);
+        const unsigned grid = (unsigned)((c->E + EPC - 1) / EPC);
+        if (lgv)
+            k_adjoint_shear<4, MODEL_ML><<<grid, EPC * G, 0, c->stream>>>(A, lam, dJdG);
+        else
+            k_adjoint_shear<4, MODEL_MS><<<grid, EPC * G, 0, c->stream>>>(A, lam, dJdG);
     }
     c->launches++;
     NB2_CUDA(c, cudaGetLastError());
