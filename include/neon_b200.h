@@ -264,7 +264,8 @@ int nb2_static_solve(nb2_ctx* ctx, const nb2_solver_options* options,
 /* ---------------------------------------------------------------------------------------- */
 
 /* Gradient of an objective J(u) with respect to the per-element shear modulus of the Gaussian
- * affine microsphere model (gaussian_affine_microsphere.cpp:23-88), at the equilibrium left by
+ * (gaussian_affine_microsphere.cpp:23-88) or Langevin (affine_microsphere.cpp:23-112) affine
+ * microsphere model, at the equilibrium left by
  * the last nb2_static_solve on this context (its displacement and Dirichlet set).  dJdu: host
  * [num_dofs]; dJdG: host [num_elements].  Solves K lambda = dJ/du (K symmetric; precision
  * NB2_FP64 or NB2_MIXED, relative tolerance `tolerance`) and evaluates
