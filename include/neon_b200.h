@@ -230,16 +230,21 @@ int nb2_pcg_solve(int32_t n, const int32_t* rowptr, const int32_t* col, const do
 
 /* Allocation-free variant of nb2_pcg_solve.  No counterpart in the reference: it exists for
  * callers that must not allocate device memory during a solve (codes that place every device
- * byte through their own pool or arena, or that must not trigger allocator growth or device
- * synchronisation mid-step).  The matrix (rowptr, col, values), b and x are DEVICE pointers the
- * caller owns; the solver's work vectors, reduction partials and scalars live in a fixed
- * workspace inside the library (NB2_NOALLOC_MAX_ROWS rows, about 4.2 MB, held by every GPU that
- * loads the library until the process exits).  n > NB2_NOALLOC_MAX_ROWS returns NB2_E_INPUT.
- * The first call on a device looks the workspace up (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share the one workspace
- * (it keeps the last call's contents; the solver re-zeroes what must start at zero), so calls
- * that overlap on the GPU race: serialise them.  stream may be NULL (legacy default stream).
- * Same algorithm, stopping rule and status codes as nb2_pcg_solve. */
+ * byte through their own pool or arena, or that must not trigger allocator growth mid-step).
+ * The matrix (rowptr, col, values), b and x are DEVICE pointers the caller owns; the solver's
+ * work vectors, reduction partials and scalars live in a fixed workspace inside the library
+ * (NB2_NOALLOC_MAX_ROWS rows, about 4.2 MB, held by every GPU that loads the library until the
+ * process exits).  n > NB2_NOALLOC_MAX_ROWS returns NB2_E_INPUT, as do row pointers that are not
+ * monotone from 0 and column indices outside [0, n); the check cannot tell a rowptr[n] larger
+ * than the caller's col/values buffers.  Each call looks the workspace up (cudaGetSymbolAddress)
+ * with the caller's device current; the first call on a device loads the library there, so make
+ * it before any stream capture.  The call allocates nothing but is not asynchronous: it blocks
+ * the host on its stream after the input check and every few dozen iterations to read the
+ * convergence flag, so it cannot run inside a stream capture.  Pass a stream created by the
+ * caller (cudaStreamNonBlocking); NULL means the legacy default stream, which synchronises with
+ * the device's other blocking streams.  All calls share the one workspace (it keeps the last
+ * call's contents; the solver re-zeroes what must start at zero), so calls that overlap on the
+ * GPU race: serialise them.  Same algorithm, stopping rule and status codes as nb2_pcg_solve. */
 #define NB2_NOALLOC_MAX_ROWS 131072
 int nb2_pcg_solve_noalloc(int32_t n, const int32_t* rowptr, const int32_t* col,
                           const double* values, const double* b, double* x, double tolerance,

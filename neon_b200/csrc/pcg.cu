@@ -1030,13 +1030,14 @@ done:
 // ---------------------------------------------------------------------------------------
 // Allocation-free PCG (nb2_pcg_solve_noalloc).
 //
-// For callers that must not allocate device memory while they run a solve -- a code that
-// places every device byte itself through its own pool or arena and forbids hidden
-// allocations, a host thread that issues work while another thread captures a stream, or a
-// long-running service that must not trigger allocator growth or device synchronisation in
-// the middle of a time step.  They pass the matrix, right-hand side and solution in device
-// memory they own; the solver's own work vectors, reduction partials and scalars live in the
-// fixed array below, which every GPU that loads this library holds until the process exits.
+// For callers that must not allocate device memory while they run a solve: a code that places
+// every device byte itself through its own pool or arena and forbids hidden allocations, or a
+// long-running service that must not trigger allocator growth in the middle of a time step.
+// They pass the matrix, right-hand side and solution in device memory they own; the solver's
+// own work vectors, reduction partials and scalars live in the fixed array below, which every
+// GPU that loads this library holds until the process exits.  The call allocates nothing, but
+// it is not asynchronous: it blocks the host on its stream after the CSR check and once every
+// kChunk iterations to read the convergence flag, so it cannot run inside a stream capture.
 // ---------------------------------------------------------------------------------------
 constexpr int kNoAllocMaxRows = NB2_NOALLOC_MAX_ROWS;
 constexpr int kNoAllocBlocks = 148 * 4;
@@ -1048,14 +1049,20 @@ static_assert(sizeof(CgScalars) <= kNoAllocScalars * sizeof(double), "scalar slo
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
-// row pointers monotone from 0, column indices in range; flag[0] = 1 on any violation
-__global__ void k_check_csr(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                            unsigned int* flag) {
-    const long long nnz = rp[n];
+// row pointers monotone from 0; flag = 1 on any violation.  Run first, and its flag read back,
+// so that the column check below never walks past a corrupt rp[n]
+__global__ void k_check_rowptr(int n, const int* __restrict__ rp, unsigned int* flag) {
+    const int nnz = rp[n];
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
         if (rp[i + 1] < rp[i] || rp[i] < 0 || rp[i + 1] > nnz) atomicOr(flag, 1u);
-    if (blockIdx.x == 0 && threadIdx.x == 0 && rp[0] != 0) atomicOr(flag, 1u);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (rp[0] != 0 || nnz < 0)) atomicOr(flag, 1u);
+}
+
+// column indices in [0, n) over [0, rp[n]) (rp already checked); flag = 1 on any violation
+__global__ void k_check_columns(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                unsigned int* flag) {
+    const long long nnz = rp[n];
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
          k += (long long)gridDim.x * blockDim.x)
         if (ci[k] < 0 || ci[k] >= n) atomicOr(flag, 1u);
@@ -1071,18 +1078,14 @@ extern "C" int nb2_pcg_solve_noalloc(int32_t n, const int32_t* rowptr, const int
     if (n <= 0 || !rowptr || !col || !values || !b || !x || maximum_iterations <= 0)
         return NB2_E_INPUT;
     if (n > kNoAllocMaxRows) return NB2_E_INPUT;  // beyond the fixed workspace
-    // device address of the fixed workspace, looked up once per device with that device
-    // current (the symbol's host-side name is not a device address)
-    static double* scratch_of_device[64] = {nullptr};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return NB2_E_CUDA;
-    if (!scratch_of_device[dev]) {
-        void* ptr = nullptr;
-        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
-            return NB2_E_CUDA;
-        scratch_of_device[dev] = static_cast<double*>(ptr);
-    }
-    double* base = scratch_of_device[dev];
+    // device address of the fixed workspace, looked up on every call with the caller's device
+    // current (the symbol's host-side name is not a device address).  The lookup allocates
+    // nothing; doing it per call keeps no pointer that a cudaDeviceReset could leave stale.
+    // The first call on a device loads the library's module there, so make it before any
+    // stream capture.
+    void* sym = nullptr;
+    if (cudaGetSymbolAddress(&sym, g_noalloc_scratch) != cudaSuccess || !sym) return NB2_E_CUDA;
+    double* base = static_cast<double*>(sym);
     double* partials = base;
     CgScalars* s = reinterpret_cast<CgScalars*>(base + kNoAllocPartials);
     double* r = base + kNoAllocPartials + kNoAllocScalars;
@@ -1095,12 +1098,21 @@ extern "C" int nb2_pcg_solve_noalloc(int32_t n, const int32_t* rowptr, const int
     // must start at zero
     if (cudaMemsetAsync(s, 0, sizeof(CgScalars), st) != cudaSuccess) return NB2_E_CUDA;
     unsigned int* flag = &s->counter[3];
-    k_check_csr<<<RB, kRedThreads, 0, st>>>(n, rowptr, col, flag);
     CgScalars hs;
-    if (cudaMemcpyAsync(&hs, s, sizeof hs, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-        return NB2_E_CUDA;
-    if (hs.counter[3] != 0) return NB2_E_INPUT;
+    auto read_flag = [&](unsigned int* out) {
+        if (cudaMemcpyAsync(&hs, s, sizeof hs, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return false;
+        *out = hs.counter[3];
+        return true;
+    };
+    unsigned int bad = 0;
+    k_check_rowptr<<<RB, kRedThreads, 0, st>>>(n, rowptr, flag);
+    if (!read_flag(&bad)) return NB2_E_CUDA;
+    if (bad != 0) return NB2_E_INPUT;
+    k_check_columns<<<RB, kRedThreads, 0, st>>>(n, rowptr, col, flag);
+    if (!read_flag(&bad)) return NB2_E_CUDA;
+    if (bad != 0) return NB2_E_INPUT;
     if (cudaMemsetAsync(s, 0, sizeof(CgScalars), st) != cudaSuccess) return NB2_E_CUDA;
     if (cudaMemcpyAsync(&s->max_iterations, &maximum_iterations, sizeof(int),
                         cudaMemcpyHostToDevice, st) != cudaSuccess)

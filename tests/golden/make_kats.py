@@ -197,4 +197,6 @@ def main(ref: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_kats.py <path to a checkout of dbeurle/neon>")
+    main(sys.argv[1])

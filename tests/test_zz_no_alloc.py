@@ -2,10 +2,12 @@
 
 It serves callers that must not allocate device memory while they solve -- codes that place
 every device byte through their own pool or arena, or that must not trigger allocator growth
-or a device synchronisation in the middle of a time step.  They hand in device buffers they
-own; the solver's work space is a fixed array inside the library.  This test owns its device
-buffers (through torch), calls the entry point twice in a row through the C-ABI and checks both
-results against the allocating entry point nb2_pcg_solve on the same systems.
+in the middle of a time step.  They hand in device buffers they own; the solver's work space is
+a fixed array inside the library.  This test owns its device buffers (through torch), calls the
+entry point twice in a row through the C-ABI and checks both results (solution, iteration count
+and final relative residual) against the allocating entry point nb2_pcg_solve on the same
+systems; then it checks the refusals (a system beyond the fixed work space, a column index out
+of range), the iteration limit status, and a call on a stream the caller created.
 
 The file name sorts last so that a run stopping at the first failure has run every other test.
 """
@@ -65,7 +67,37 @@ def test_noalloc_pcg_matches_allocating_entry_point():
         x = d_x.cpu().numpy()
         assert rel_err(x, x_ref) < 1e-9, call
         assert abs(it.value - cg.iterations) <= max(2, 0.02 * cg.iterations)
+        assert err.value <= tol and cg.error <= tol
+        if it.value == cg.iterations:  # same iterates: the same final residual
+            assert abs(err.value - cg.error) <= 1e-6 * cg.error
     # a system beyond the fixed work space is refused, not run
     st = L.nb2_pcg_solve_noalloc(131072 + 1, d_rp.data_ptr(), d_col.data_ptr(), d_val.data_ptr(),
                                  d_b.data_ptr(), d_x.data_ptr(), tol, maxit, None, None, None)
     assert st == api.E_INPUT
+    # a column index outside [0, n) (inside the caller's buffer) is refused before any solve
+    bad_col = col.copy()
+    bad_col[len(bad_col) // 2] = n
+    d_bad = torch.from_numpy(bad_col).to(dev)
+    torch.cuda.synchronize()
+    st = L.nb2_pcg_solve_noalloc(n, d_rp.data_ptr(), d_bad.data_ptr(), d_val.data_ptr(),
+                                 d_b.data_ptr(), d_x.data_ptr(), tol, maxit, None, None, None)
+    assert st == api.E_INPUT
+    # the iteration limit gives the same status as the allocating entry point
+    it = C.c_int32()
+    st = L.nb2_pcg_solve_noalloc(n, d_rp.data_ptr(), d_col.data_ptr(), d_val.data_ptr(),
+                                 d_b.data_ptr(), d_x.data_ptr(), tol, 3, None, C.byref(it), None)
+    assert st == api.E_CG_MAXIT and it.value == 3
+    with pytest.raises(api.ComputationalError):
+        api.ConjugateGradient(tol, 3).solve((rp, col, K), np.zeros(n), b)
+    # on a stream the caller created, after work queued on it
+    s = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(s):
+        d_b2 = d_b * 2.0
+        d_x2 = torch.zeros(n, dtype=torch.float64, device=dev)
+    err = C.c_double()
+    st = L.nb2_pcg_solve_noalloc(n, d_rp.data_ptr(), d_col.data_ptr(), d_val.data_ptr(),
+                                 d_b2.data_ptr(), d_x2.data_ptr(), tol, maxit,
+                                 C.c_void_p(s.cuda_stream), None, C.byref(err))
+    assert st == api.OK
+    s.synchronize()
+    assert rel_err(d_x2.cpu().numpy(), 2.0 * x_ref) < 1e-9
