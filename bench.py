@@ -180,6 +180,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
+def workload_name(size):
+    """The workload string both arms report (the same config: update + K + f_int of the J2 mesh
+    in the same plastic state)."""
+    return (f"J2 hex8 {size}^3 (sigma_y=200, E=200e3, nu=0.3, H=1e3), fused update+K+f_int, "
+            f"plastic state")
+
+
 def algorithmic_work(mesh_size, nnz, n_nodes, E, nqp, fp64=True):
     """Canonical algorithmic work of one J2 hex8 assembly (bytes, flops): K written once,
     connectivity, X, u, f_int, J2 state read (7 FP64) and written (7 FP64) per point; FLOPs
@@ -228,6 +235,48 @@ def cpu_baseline_sample(threads=None, target_seconds=15.0):
                       f"plastic state) x{reps}, {cores} OpenMP threads"}
 
 
+def cpu_newton_baselines(args):
+    """Newton-step wall times of the oracle (neon's CPU path restated: OpenMP assembly with
+    binary-search atomics, RCM + Jacobi-PCG) on this host, all OpenMP threads: C1 in full, the
+    first `cpu_c2_increments` increments of C2, the first increment of C3 (unless skipped) and
+    the C3 PCG time per iteration on the assembled, Dirichlet-constrained first tangent."""
+    from oracle import binding as ob
+    from neon_b200 import problem as P
+    out = {"cores": ob.max_threads(), "cpu": ob._cpu_model(), "kind": "port"}
+
+    def solve(pr, label):
+        t0 = time.perf_counter()
+        rep, u, _, lg, _ = ob.static_solve(pr)
+        dt = time.perf_counter() - t0
+        nit = max(1, int(rep["newton_iterations"]))
+        cg = int(lg[:, 2].sum()) if len(lg) else 0
+        log(f"cpu {label}: {dt:.1f} s, {nit} Newton iterations, {cg} CG iterations")
+        return {"status": int(rep["status"]), "seconds": dt, "load_steps": int(rep["load_steps"]),
+                "newton_iterations": nit, "cg_iterations": cg, "newton_step_s": dt / nit}
+
+    out["c1_full"] = solve(P.config_c1(20), "C1 20^3 full")
+    pr = P.config_c2(64)
+    pr.options.period = args.cpu_c2_increments * pr.options.initial
+    out["c2"] = solve(pr, f"C2 64^3 {args.cpu_c2_increments} increment(s)")
+    out["c2"]["increments"] = args.cpu_c2_increments
+    if not args.cpu_skip_c3:
+        pr = P.config_c3(100)
+        pr.options.period = pr.options.initial
+        out["c3_first_increment"] = solve(pr, "C3 100^3 first increment")
+        # the PCG per iteration on the first tangent (a fixed count of iterations)
+        om = ob.OracleMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+        om.update(np.zeros(om.ndofs))
+        K = om.assemble()
+        rp, col = om.pattern()
+        its = 20
+        secs, t_perm = ob.cg_sample_seconds(rp, col, K, np.ones(om.ndofs), its)
+        out["c3_pcg"] = {"iterations_timed": its, "ms_per_iteration": 1e3 * secs / its,
+                         "rcm_permutation_s": t_perm,
+                         "note": "Jacobi-PCG iterations on P^T K P; the per-solve RCM "
+                                 "permutation (rcm_permutation_s) is paid once per solve"}
+    return out
+
+
 def run_reference(args):
     """Reference arm: the reference's CPU algorithm (oracle port; the reference itself cannot be
     built here) on the same config, all host threads."""
@@ -267,8 +316,10 @@ def run_reference(args):
             "steps": steps, "warmup": warm, "ms_per_step": 1e3 * dt / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"J2 hex8 {args.size}^3 assembly (update + K + f_int)",
-                       "elements": E, "dofs": om.ndofs, "nnz": int(om.nnz)},
+            "config": {"workload": workload_name(args.size),
+                       "elements": E, "dofs": om.ndofs, "nnz": int(om.nnz),
+                       "parallelism": "replicas x1",
+                       "l2": "inputs larger than L2 (K 1.96 GB, state 0.45 GB)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{steps} full assemblies of the {args.size}^3 mesh on "
                                        f"{cores} OpenMP threads"},
@@ -286,6 +337,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=100)
     ap.add_argument("--newton-load-steps", type=int, default=2)
+    ap.add_argument("--newton-cyclic-increments", type=int, default=24,
+                    help="increments of the cyclic segment (80 = the whole 20-step cycle)")
     ap.add_argument("--no-newton", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -293,7 +346,16 @@ def main():
     ap.add_argument("--cg-iterations", type=int, default=200)
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-size", type=int, default=48)
+    ap.add_argument("--cpu-newton", action="store_true",
+                    help="only time the oracle's Newton steps (C1, C2, C3) and print them")
+    ap.add_argument("--cpu-c2-increments", type=int, default=1)
+    ap.add_argument("--cpu-skip-c3", action="store_true")
     args = ap.parse_args()
+    if args.cpu_newton:
+        print(json.dumps({"cpu_newton": cpu_newton_baselines(args)}), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
 
@@ -356,6 +418,21 @@ def main():
     if dist:
         t_max = max_over_ranks(t_asm, dist)
     value = world * E / t_max
+    # the same assembly with the colour-partitioned, bit-reproducible scatter (the Newton
+    # driver's mode), outside the headline's timed region
+    mesh.set_scatter_mode(api.SCATTER_COLOURED)
+    for _ in range(warmup):
+        assembly_step()
+    col_ms = []
+    for _ in range(args.steps):
+        assembly_step()
+        ev1.synchronize()
+        col_ms.append(ev0.elapsed_time(ev1))
+    mesh.set_scatter_mode(api.SCATTER_RED)
+    coloured = {"ms_per_step": sum(col_ms) / len(col_ms),
+                "elements_per_s": E / (sum(col_ms) / len(col_ms) * 1e-3),
+                "note": "one launch per element colour, first term stored, later colours added: "
+                        "bit-reproducible K and f_int (nb2_static_solve always uses it)"}
 
     # roofline of the dominant kernel (the fused element kernel)
     peaks = {}
@@ -407,6 +484,9 @@ def main():
         newton = newton_comparison(api, P, args, mesh)
 
     log("newton done")
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_timing(api, P, args)
     batched = None
     if not args.no_batch and args.batch_instances > 0:
         batched = batched_comparison(api, P, args)
@@ -419,15 +499,16 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": warmup, "ms_per_step": t_max * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"J2 hex8 {args.size}^3 (sigma_y=200, E=200e3, nu=0.3, "
-                                   f"H=1e3), fused update+K+f_int, plastic state",
+            "config": {"workload": workload_name(args.size),
                        "elements": E, "dofs": mesh.ndofs, "nnz": mesh.nnz,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (K 1.96 GB, state 0.45 GB)"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "scatter": "red.global.add into zeroed K and f_int (NB2_SCATTER_RED, the default "
+                       "for standalone assembly)",
+            "coloured_scatter": coloured, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "timed_region_ms": region_ms, "clocks": clock_info,
             "fp32_fma_peak_tflops": fp32_peak / 1e12, "pcg": pcg, "newton": newton,
-            "batched": batched}
+            "adjoint": adjoint, "batched": batched}
     if rank == 0:
         print(json.dumps(line), flush=True)
     mesh.close()
@@ -525,18 +606,28 @@ def _rel(a, b):
 
 
 def newton_comparison(api, P, args, mesh_unused):
-    """FP64 vs mixed device Newton on the 100^3 J2 mesh: the first load increment (elastic
-    range) and the first `newton_load_steps` increments (yielding).  The J2 update of the
-    reference mutates the plastic strain at every Newton iteration, so once points yield the
-    converged displacement depends on the Newton path: a perturbation of the iterates at
-    round-off level moves points across the yield surface.  `fp64_rerun` measures that floor
-    with the FP64 path against itself under the same settings (the order of K's reductions
-    differs between runs), `fp64_reproducibility` at a 10x tighter CG tolerance."""
+    """FP64 vs mixed device Newton on the 100^3 J2 mesh, Newton-step seconds = the segment's
+    wall time over its Newton iterations (update, assembly or stored tangent, Dirichlet, PCG to
+    rtol 1e-10, norms):
+      first_increment  the first load increment (elastic range);
+      yielding         the first `newton_load_steps` increments (points yield);
+      cyclic           the first `newton_cyclic_increments` increments of the 80-increment
+                       cycle (24 = t in [0, 6]: past the load reversal at t = 5, where the top
+                       face starts to unload); 80 runs the whole cycle.
+    The reference's J2 update mutates the plastic strain at every Newton iteration, so once
+    points yield the converged displacement depends on the Newton path.  The FP64 path is bit
+    reproducible (fixed-order assembly and reductions): `fp64_rerun_rel_err_u` is that check;
+    `fp64_rtol_sensitivity_rel_err_u` (rtol 1e-10 vs 1e-11) measures how far a perturbation of
+    the iterates at the CG tolerance moves the converged displacement, the scale any other
+    solver meets; the mixed path is also compared at rtol 1e-12 on both paths."""
     delta = 1e-3
     out = {"mixed_method": "reliable-update PCG: FP32 matrix-free tangent, FP64 residual "
                            f"replacement every {delta:g} reduction, same rtol as FP64",
            "segments": {}}
-    for name, steps in (("first_increment", 1), ("yielding", args.newton_load_steps)):
+    segs = [("first_increment", 1), ("yielding", args.newton_load_steps)]
+    if args.newton_cyclic_increments > 0:
+        segs.append(("cyclic", args.newton_cyclic_increments))
+    for name, steps in segs:
         u64, r64 = _newton_run(api, P, args.size, steps, api.FP64)
         log(f"newton {name} fp64: {r64['seconds_total']:.2f} s")
         u32, r32 = _newton_run(api, P, args.size, steps, api.MIXED, delta)
@@ -546,17 +637,60 @@ def newton_comparison(api, P, args, mesh_unused):
                "newton_step_speedup": r64["newton_step_s"] / max(r32["newton_step_s"], 1e-12),
                "solve_speedup": r64["seconds_total"] / max(r32["seconds_total"], 1e-12)}
         if name == "yielding":
-            # the floor any comparison meets once points yield: the FP64 path against itself,
-            # rerun with the same settings (K's reductions change its last bits, points on the
-            # yield surface amplify them) and at a 10x tighter CG tolerance
             u64r, _ = _newton_run(api, P, args.size, steps, api.FP64)
             seg["fp64_rerun_rel_err_u"] = _rel(u64r, u64)
+            seg["fp64_rerun_bitwise_equal"] = bool(np.array_equal(u64r, u64))
             u64b, _ = _newton_run(api, P, args.size, steps, api.FP64, cg_tol=1e-11)
-            seg["fp64_reproducibility_rel_err_u"] = _rel(u64b, u64)
+            seg["fp64_rtol_sensitivity_rel_err_u"] = _rel(u64b, u64)
+            # both paths at a tighter CG tolerance
+            t64, q64 = _newton_run(api, P, args.size, steps, api.FP64, cg_tol=1e-12)
+            t32, q32 = _newton_run(api, P, args.size, steps, api.MIXED, delta, cg_tol=1e-12)
+            seg["rtol_1e-12"] = {
+                "fp64": q64, "mixed": q32, "mixed_rel_err_u": _rel(t32, t64),
+                "newton_step_speedup": q64["newton_step_s"] / max(q32["newton_step_s"], 1e-12)}
+            log(f"newton {name} rtol 1e-12: mixed err {seg['rtol_1e-12']['mixed_rel_err_u']:.2e}")
         out["segments"][name] = seg
-    y = out["segments"]["yielding"]
-    out["newton_step_speedup"] = y["newton_step_speedup"]
-    out["mixed_rel_err_u"] = y["mixed_rel_err_u"]
+    main = out["segments"]["cyclic" if "cyclic" in out["segments"] else "yielding"]
+    out["newton_step_s_fp64"] = main["fp64"]["newton_step_s"]
+    out["newton_step_s_mixed"] = main["mixed"]["newton_step_s"]
+    out["newton_step_speedup"] = main["newton_step_speedup"]
+    out["mixed_rel_err_u"] = main["mixed_rel_err_u"]
+    return out
+
+
+def adjoint_timing(api, P, args):
+    """Config 4 at 48^3: the forward solve and the adjoint gradient dJ/dG_e of
+    J = 1/2 |u_top - u_target|^2 over all 110,592 per-element shear moduli, FP64 and with the
+    FP32-bulk inner solves; seconds of each and the relative difference of the two gradients.
+    The central-difference check of the gradient is in tests/test_gpu_adjoint.py."""
+    n = args.adjoint_size
+    target = P.config_c4(n, seed_field=99)
+    sm_t = api.StaticMatrix(target)
+    u_target = sm_t.solve()
+    sm_t.mesh.close()
+    pr = P.config_c4(n, seed_field=7)
+    sm = api.StaticMatrix(pr)
+    t0 = time.perf_counter()
+    u = sm.solve()
+    t_fwd = time.perf_counter() - t0
+    top = np.unique(pr.mesh.faces["top"].reshape(-1))
+    dofs = (3 * top[:, None] + np.arange(3)).reshape(-1)
+    g = np.zeros_like(u)
+    g[dofs] = u[dofs] - u_target[dofs]
+    out = {"mesh": f"{n}^3 hex8 ({pr.mesh.num_elements} elements, {3 * pr.mesh.num_nodes} DOFs)",
+           "forward_solve_s": t_fwd, "forward_newton_iterations":
+           int(sm.report["newton_iterations"])}
+    grads = {}
+    for name, prec in (("fp64", api.FP64), ("mixed", api.MIXED)):
+        sm.mesh.adjoint_shear_gradient(g, prec, 1e-10)  # warm (buffers, graphs)
+        t0 = time.perf_counter()
+        grads[name] = sm.mesh.adjoint_shear_gradient(g, prec, 1e-10)
+        dt = time.perf_counter() - t0
+        out[name] = {"adjoint_s": dt, "inner_iterations": int(sm.mesh.adjoint_iterations)}
+        log(f"adjoint {name}: {dt * 1e3:.1f} ms")
+    out["mixed_vs_fp64_rel_err_grad"] = _rel(grads["mixed"], grads["fp64"])
+    out["adjoint_over_forward"] = out["fp64"]["adjoint_s"] / max(t_fwd, 1e-12)
+    sm.mesh.close()
     return out
 
 

@@ -157,6 +157,24 @@ int nb2_destroy(nb2_ctx* ctx);
 int nb2_last_error(const nb2_ctx* ctx, char* buffer, size_t size);
 /* Run all work of this context on a caller stream (cudaStream_t passed as void*). */
 int nb2_set_stream(nb2_ctx* ctx, void* stream);
+
+/* How element passes add element contributions into K and f_int (hex8, FP64).  No reference
+ * counterpart: neon adds with OpenMP atomics (thread_safe_plugin.hpp:7-23), so its sums run in
+ * a thread-dependent order.
+ *   NB2_SCATTER_RED       (default for nb2_update_internal_variables / nb2_assemble /
+ *                         nb2_update_assemble_device) red.global.add into zeroed arrays: the
+ *                         fastest; the order of the additions, and so the last bits, can
+ *                         change from run to run.
+ *   NB2_SCATTER_COLOURED  one launch per element colour (elements of a colour share no node):
+ *                         every entry's first term is stored and the later colours' terms added,
+ *                         in colour order, so the same inputs give bit-identical K and f_int.
+ * nb2_static_solve always uses the coloured scatter, whatever this setting: its Newton iterates,
+ * CG and solution are then bit-reproducible (the element passes are ~1% of a Newton step).
+ * tet4 meshes, the anisotropic microsphere tangent, FP32 K and batched instances always use
+ * red.global.add. */
+#define NB2_SCATTER_RED 0
+#define NB2_SCATTER_COLOURED 1
+int nb2_set_scatter_mode(nb2_ctx* ctx, int32_t mode);
 int nb2_get_sizes(const nb2_ctx* ctx, int32_t* num_dofs, int64_t* nnz, int64_t* num_blocks);
 /* Number of kernels this library launched for the context so far. */
 int nb2_launch_count(const nb2_ctx* ctx, int64_t* launches);
@@ -210,6 +228,27 @@ int nb2_get_quadrature_values(nb2_ctx* ctx, int32_t which, double* out);
  * 2 plastic strain [num_nodes][9], 3 accumulated plastic strain [num_nodes], 4 von Mises stress
  * [num_nodes].  Host output. */
 int nb2_nodal_averaged_variable(nb2_ctx* ctx, int32_t which, double* out);
+
+/* Non-follower loads (nonfollower_load_boundary, mechanics/solid/boundary/nonfollower_load.cpp:
+ * 12-121): the nodal external-force vector of one load boundary per unit load value, in the
+ * initial configuration, computed on the device.  The Newton driver scales it by the boundary's
+ * time table (pass it as a weighted table in nb2_static_solve's nodal_forces).
+ *   NB2_LOAD_TRACTION   surface_load::external_force (mesh/boundary/neumann.hpp:69-133): f[3a+k]
+ *                       = sum_q w N_a |X,xi x X,eta| for the given component k;
+ *   NB2_LOAD_PRESSURE   pressure::external_force (pressure.cpp:9-37): f[3a+i] = -sum_q w N_a n_i
+ *                       |X,xi x X,eta|, n the unit normal X,xi x X,eta / |..| (positive pressure
+ *                       compresses the surface; component is ignored);
+ *   NB2_LOAD_BODY_FORCE volume_load::external_force (neumann.hpp:135-192) over the context's
+ *                       elements: f[3a+k] = sum_q w N_a det(X dN).
+ * faces [num_faces][nodes_per_face]: quad4 (4-point rule, or the 1-point rule when
+ * reduced_quadrature is set) or tri3 (1-point rule) boundary faces in neon's local node order
+ * (surface loads only; NULL for a body force).  f_out [num_dofs] (host) is overwritten. */
+#define NB2_LOAD_TRACTION 0
+#define NB2_LOAD_PRESSURE 1
+#define NB2_LOAD_BODY_FORCE 2
+int nb2_nonfollower_load(nb2_ctx* ctx, int32_t kind, int32_t component, const int32_t* faces,
+                         int32_t num_faces, int32_t nodes_per_face, int32_t reduced_quadrature,
+                         double* f_out);
 
 /* static_matrix::enforce_dirichlet_conditions (static_matrix.hpp:279-320) on host CSR values
  * laid out as nb2_export_pattern: zero row and column of each listed DOF, keep the diagonal,

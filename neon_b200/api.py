@@ -28,6 +28,8 @@ OK, E_NEG_DETJ, E_NAN, E_RETURN_MAP, E_CG_MAXIT, E_CG_BREAKDOWN, E_TIMEOUT, E_IN
     E_NEWTON_MAXIT, E_CUTBACK_LIMIT = range(11)
 RECOVERABLE = {E_NEG_DETJ, E_NAN, E_RETURN_MAP, E_CG_MAXIT, E_CG_BREAKDOWN, E_NEWTON_MAXIT}
 FP64, MIXED = 0, 1
+# element-pass scatter modes (nb2_set_scatter_mode)
+SCATTER_RED, SCATTER_COLOURED = 0, 1
 
 
 class ComputationalError(RuntimeError):
@@ -92,6 +94,7 @@ _SIGS = {
     "nb2_destroy": (C.c_int, [P]),
     "nb2_last_error": (C.c_int, [P, C.c_char_p, C.c_size_t]),
     "nb2_set_stream": (C.c_int, [P, P]),
+    "nb2_set_scatter_mode": (C.c_int, [P, C.c_int32]),
     "nb2_get_sizes": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                                 C.POINTER(C.c_int64)]),
     "nb2_launch_count": (C.c_int, [P, C.POINTER(C.c_int64)]),
@@ -105,6 +108,8 @@ _SIGS = {
     "nb2_apply_tangent_fp32": (C.c_int, [P, P, P]),
     "nb2_get_quadrature_values": (C.c_int, [P, C.c_int32, P]),
     "nb2_nodal_averaged_variable": (C.c_int, [P, C.c_int32, P]),
+    "nb2_nonfollower_load": (C.c_int, [P, C.c_int32, C.c_int32, P, C.c_int32, C.c_int32,
+                                       C.c_int32, P]),
     "nb2_apply_dirichlet": (C.c_int, [P, P, C.c_int32, P, P]),
     "nb2_pcg_solve": (C.c_int, [C.c_int32, P, P, P, P, P, C.c_double, C.c_int32,
                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
@@ -264,6 +269,17 @@ class SolidMesh:
         _check(lib().nb2_nodal_averaged_variable(self.h, idx, out.ctypes.data), self.h, which)
         return out.reshape(-1, k) if k > 1 else out
 
+    def nonfollower_load(self, kind, component=0, faces=None, reduced=False):
+        """The nodal vector [3N] per unit value of a traction / pressure on boundary faces or of
+        a body force over the elements, computed on the device (nb2_nonfollower_load)."""
+        out = np.zeros(self.ndofs)
+        fc = None if faces is None else np.ascontiguousarray(faces, dtype=np.int32)
+        nf, npf = (0, 0) if fc is None else (fc.shape[0], fc.shape[1])
+        _check(lib().nb2_nonfollower_load(self.h, int(kind), int(component), _ptr(fc), nf, npf,
+                                          int(bool(reduced)), out.ctypes.data), self.h,
+               "nonfollower_load")
+        return out
+
     def apply_dirichlet(self, dofs, K, b):
         dofs = np.ascontiguousarray(dofs, dtype=np.int32)
         _check(lib().nb2_apply_dirichlet(self.h, dofs.ctypes.data, len(dofs), K.ctypes.data,
@@ -302,6 +318,12 @@ class SolidMesh:
                                       int(maximum_iterations), C.byref(it), C.byref(err)),
                self.h, "solve_device")
         return it.value, err.value
+
+    def set_scatter_mode(self, mode: int):
+        """SCATTER_RED (fast, run-to-run last-bit differences) or SCATTER_COLOURED (one launch
+        per element colour, bit-reproducible) for this mesh's update / assembly calls; the
+        Newton driver always uses the coloured scatter."""
+        _check(lib().nb2_set_scatter_mode(self.h, int(mode)), self.h, "set_scatter_mode")
 
     def set_stream(self, stream_handle: int):
         _check(lib().nb2_set_stream(self.h, stream_handle), self.h, "set_stream")
@@ -398,16 +420,27 @@ class StaticMatrix:
         self.log = None
         self.displacement = None
 
+    def external_force_tables(self):
+        """The problem's nodal-force tables plus its non-follower loads, their nodal vectors
+        computed on the device."""
+        from .problem import load_tables
+        tables = list(self.problem.nodal_forces)
+        for spec in self.problem.loads:
+            f = self.mesh.nonfollower_load(spec.kind, spec.component, spec.faces, spec.reduced)
+            tables.append(load_tables(spec, f))
+        return tables
+
     def solve(self, max_log=100000, raise_on_error=True):
         keep = []
         dt = _tables(self.problem.dirichlet, keep)
-        nf = _tables(self.problem.nodal_forces, keep)
+        forces = self.external_force_tables()
+        nf = _tables(forces, keep)
         u = np.zeros(self.mesh.ndofs)
         rep = SolveReport()
         log = (NewtonLog * max_log)()
         st = lib().nb2_static_solve(self.mesh.h, C.byref(self.options), C.cast(dt, P),
                                     len(self.problem.dirichlet), C.cast(nf, P),
-                                    len(self.problem.nodal_forces), u.ctypes.data, C.byref(rep),
+                                    len(forces), u.ctypes.data, C.byref(rep),
                                     C.cast(log, P), max_log)
         self.displacement = u
         self.report = {k: getattr(rep, k) for k, _ in SolveReport._fields_}

@@ -16,7 +16,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libneon_b200.so")
-SOURCES = ["api.cu", "batch.cu", "elements.cu", "pattern.cu", "pcg.cu", "post.cu", "probe.cu"]
+SOURCES = ["api.cu", "batch.cu", "elements.cu", "loads.cu", "pattern.cu", "pcg.cu", "post.cu",
+           "probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -228,9 +228,12 @@ int nb2_destroy(nb2_ctx* c) {
                     c->ep_old, c->epbar_old, c->sig, c->dpar,   c->detF,      c->cg_x,
                     c->cg_r,   c->cg_p,   c->cg_q,   c->cg_inv, c->cg32_x,    c->cg32_r,
                     c->cg32_p, c->cg32_q, c->cg32_inv, c->partials, c->cgs,   c->norms,
-                    c->status};
+                    c->status, c->corder, c->kfirst, c->ffirst};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (cudaEvent_t ev : c->zev)
+        if (ev) cudaEventDestroy(ev);
+    if (c->zstream) cudaStreamDestroy(c->zstream);
     if (c->h_cgs) cudaFreeHost(c->h_cgs);
     if (c->h_norms) cudaFreeHost(c->h_norms);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -252,6 +255,12 @@ int nb2_set_stream(nb2_ctx* c, void* stream) {
     if (c->own_stream) cudaStreamDestroy(c->stream);
     c->stream = (cudaStream_t)stream;
     c->own_stream = false;
+    return NB2_OK;
+}
+
+int nb2_set_scatter_mode(nb2_ctx* c, int32_t mode) {
+    if (!c || (mode != NB2_SCATTER_RED && mode != NB2_SCATTER_COLOURED)) return NB2_E_INPUT;
+    c->scatter = mode;
     return NB2_OK;
 }
 
@@ -987,7 +996,9 @@ extern "C" int nb2_static_solve(nb2_ctx* c, const nb2_solver_options* options,
     nw.load.init(options->period, options->initial_increment, options->minimum_increment,
                  options->maximum_increment, options->adaptive != 0, history);
     c->error.clear();
+    c->newton_scatter = true;  // bit-reproducible Newton: coloured element passes
     int st = nw.solve();
+    c->newton_scatter = false;
     if (u_out) {
         cudaMemcpyAsync(u_out, c->u, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream);
         cudaStreamSynchronize(c->stream);

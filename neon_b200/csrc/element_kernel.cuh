@@ -8,8 +8,11 @@
 //            reduce-scatter, so lane l ends with node l's force);
 //   phase 2  hex8 in FP64 (every model but the anisotropic microspheres): each warp forms the
 //            64 blocks of its elements, one element at a time, as 8x8 node x node tiles with
-//            FP64 mma.sync, stages them in shared memory and adds them to K with red.global.add,
-//            consecutive lanes on consecutive entries of a block;
+//            FP64 mma.sync, stages them in shared memory and writes them to K, consecutive
+//            lanes on consecutive entries of a block: in a colour-partitioned pass (A.order) a
+//            block's first term is stored and the later colours' terms added, so no entry ever
+//            has two writers at once and the sums run in colour order; otherwise each term is
+//            added with red.global.add into a zeroed K;
 //            otherwise: each lane accumulates its upper-triangular 3x3 blocks over the points in
 //            Real precision, in passes of at most 3 blocks (fewer live registers), and adds them
 //            (and their mirrored blocks) to K with red.global.add.
@@ -64,7 +67,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
     const int tid = threadIdx.x;
     const int le = tid / G;
     const int lane = tid % G;
-    const long long e = (long long)blockIdx.x * EPC + le;
+    const long long e = element_at(A, (long long)blockIdx.x * EPC + le);
     const bool valid = element_enabled(A, e);
 
     for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
@@ -102,10 +105,10 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
         for (int c = 0; c < 6; ++c) o.sig[c] = o.N[c] = 0.0;
         double Ji[9], s = 0.0;
         if (active) {
-            const double w = (NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0);
             const long long q = e * NQ + l;
-            // one pass over the nodes: F = x dN, F0 = X dN and U = (x - X) dN; then
-            // H = U F0^-1 (= sum_a (x_a - X_a) (x) (dN_a F0^-1), submesh.cpp:225-231)
+            // one pass over the nodes: F0 = X dN and U = (x - X) dN, then the current
+            // Jacobian F = x dN = F0 + U, H = U F0^-1 (= sum_a (x_a - X_a) (x) (dN_a F0^-1),
+            // submesh.cpp:225-231); without the update only F
             double Fc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             double F0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             double U[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -117,21 +120,36 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         const double d = sdN[l][a][k];
-                        Fc[i * 3 + k] += xi * d;
                         if constexpr (kCon) {
                             F0[i * 3 + k] += Xi * d;
                             U[i * 3 + k] += di * d;
+                        } else {
+                            Fc[i * 3 + k] += xi * d;
                         }
                     }
                 }
             if constexpr (kCon) {
+#pragma unroll
+                for (int i = 0; i < 9; ++i) Fc[i] = F0[i] + U[i];
+            }
+            // J^-1 and w det J of the current configuration (submesh.cpp:82-160)
+            const double detJ = inv3_det(Fc, Ji);
+            s = ((NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0)) * detJ;
+            if constexpr (kCon) {
                 double F0i[9];
-                inv3(F0, F0i);
+                const double det0 = inv3_det(F0, F0i);
                 double Hm[9];
                 matmul3(U, F0i, Hm);
+                // F_def = F F0^-1 (submesh.cpp:233); the small-strain models need only its
+                // determinant, det F / det F0
                 double Fd[9];
-                matmul3(Fc, F0i, Fd);
-                const double detF = det3(Fd);
+                double detF;
+                if constexpr (kFinite) {
+                    matmul3(Fc, F0i, Fd);
+                    detF = det3(Fd);
+                } else {
+                    detF = detJ / det0;
+                }
                 if (signbit(detF)) {
                     const unsigned long long key = ((unsigned long long)q << 32) |
                                                    (unsigned long long)__float_as_uint((float)detF);
@@ -189,8 +207,6 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                     for (int c = 0; c < 6; ++c) o.N[c] = A.dpar[(3 + c) * n + q];
                 }
             }
-            inv3(Fc, Ji);
-            s = w * det3(Fc);
         }
         if constexpr (kStiff || kForce) {
             // per node a: L_a = J^-T dN_a (stored for the stiffness phase) and g_a = s sigma L_a
@@ -292,13 +308,21 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
 
     if constexpr (kForce) {
         if (valid) {
+            const unsigned fm = A.ffirst ? A.ffirst[e] : 0u;
 #pragma unroll
             for (int j = 0; j < NG; ++j) {
                 const int a = lane + j * G;
                 if (a < NPE) {
-                    atomicAdd(&A.fint[3ll * node[j] + 0], fown[j][0]);
-                    atomicAdd(&A.fint[3ll * node[j] + 1], fown[j][1]);
-                    atomicAdd(&A.fint[3ll * node[j] + 2], fown[j][2]);
+                    double* fa = &A.fint[3ll * node[j]];
+                    if ((fm >> a) & 1u) {  // this node's first term in colour order
+                        fa[0] = fown[j][0];
+                        fa[1] = fown[j][1];
+                        fa[2] = fown[j][2];
+                    } else {
+                        atomicAdd(&fa[0], fown[j][0]);
+                        atomicAdd(&fa[1], fown[j][1]);
+                        atomicAdd(&fa[2], fown[j][2]);
+                    }
                 }
             }
         }
@@ -320,10 +344,11 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
 #pragma unroll 1
         for (int j = 0; j < 4; ++j) {
             const int le2 = warp * 4 + j;
-            const long long e2 = (long long)blockIdx.x * EPC + le2;
+            const long long e2 = element_at(A, (long long)blockIdx.x * EPC + le2);
             if (!element_enabled(A, e2)) continue;  // the same for all lanes of the warp
             const int* slot = A.slot + e2 * (NPE * NPE);
             const int sl0 = slot[lane32], sl1 = slot[32 + lane32];
+            const unsigned long long kf = A.kfirst ? A.kfirst[e2] : 0ull;
             double Lq[2][3], cl[2], cm[2], cb[2];
 #pragma unroll
             for (int st = 0; st < 2; ++st) {
@@ -409,7 +434,12 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                 const int idx = it * 32 + lane32;
                 const int blk = idx / 9;
                 const long long sab = sSl[warp][blk];
-                atomicAdd(&Kp[9 * sab + (idx - 9 * blk)], sKe[warp][idx + (blk >> 4)]);
+                const double v = sKe[warp][idx + (blk >> 4)];
+                double* kp = &Kp[9 * sab + (idx - 9 * blk)];
+                if ((kf >> blk) & 1ull)  // the block's first term in colour order
+                    *kp = v;
+                else
+                    atomicAdd(kp, v);
             }
             __syncwarp();
         }

@@ -92,6 +92,25 @@ __device__ __forceinline__ void inv3(const double* m, double* r) {
     r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
 }
 
+// inverse as inv3, returning the determinant of m (the cofactor expansion along the first column)
+__device__ __forceinline__ double inv3_det(const double* m, double* r) {
+    double c00 = m[4] * m[8] - m[5] * m[7];
+    double c10 = m[7] * m[2] - m[8] * m[1];
+    double c20 = m[1] * m[5] - m[2] * m[4];
+    double det = c00 * m[0] + c10 * m[3] + c20 * m[6];
+    double id = 1.0 / det;
+    r[0] = c00 * id;
+    r[1] = c10 * id;
+    r[2] = c20 * id;
+    r[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+    r[4] = (m[8] * m[0] - m[6] * m[2]) * id;
+    r[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    r[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+    r[7] = (m[6] * m[1] - m[7] * m[0]) * id;
+    r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+    return det;
+}
+
 __device__ __forceinline__ void matmul3(const double* a, const double* b, double* c) {
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -499,7 +518,14 @@ __device__ __forceinline__ void report_status(const ElementArgs& A, long long e,
 
 // batched solves compute only the elements of the instances still iterating
 __device__ __forceinline__ bool element_enabled(const ElementArgs& A, long long e) {
-    return e < A.E && (A.inst_on == nullptr || A.inst_on[A.e_inst[e]] != 0);
+    return e >= 0 && e < A.E && (A.inst_on == nullptr || A.inst_on[A.e_inst[e]] != 0);
+}
+
+// the element at position pos of this launch: the pos-th element of the launch's colour in a
+// colour-partitioned pass, else element pos; -1 past the end
+__device__ __forceinline__ long long element_at(const ElementArgs& A, long long pos) {
+    if (pos >= A.ecount) return -1;
+    return A.order ? (long long)A.order[pos] : A.ebegin + pos;
 }
 
 // D += A B for one 8x8x4 FP64 tile (mma.sync m8n8k4, row.col): lane l holds A[l/4][l%4],
@@ -534,7 +560,7 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
     const int tid = threadIdx.x;
     const int le = tid / G;
     const int lane = tid % G;
-    const long long e = (long long)blockIdx.x * EPC + le;
+    const long long e = element_at(A, (long long)blockIdx.x * EPC + le);
     const bool valid = element_enabled(A, e);
     for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
         (&sdN[0][0][0])[i] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
@@ -642,6 +668,7 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
     }
     __syncthreads();
     if (!valid) return;
+    const unsigned fm = A.ffirst ? A.ffirst[e] : 0u;
 #pragma unroll
     for (int j = 0; j < (NPE + G - 1) / G; ++j) {
         int a = lane + j * G;
@@ -653,9 +680,16 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
                 f1 += sY[le][l][3 * a + 1];
                 f2 += sY[le][l][3 * a + 2];
             }
-            atomicAdd(&y[3ll * node[j] + 0], f0);
-            atomicAdd(&y[3ll * node[j] + 1], f1);
-            atomicAdd(&y[3ll * node[j] + 2], f2);
+            double* ya = &y[3ll * node[j]];
+            if ((fm >> a) & 1u) {  // first term of this node in colour order
+                ya[0] = f0;
+                ya[1] = f1;
+                ya[2] = f2;
+            } else {
+                atomicAdd(&ya[0], f0);
+                atomicAdd(&ya[1], f1);
+                atomicAdd(&ya[2], f2);
+            }
         }
     }
 }
@@ -1057,10 +1091,16 @@ static int upload_tables(nb2_ctx* c) {
     return NB2_OK;
 }
 
+// elements a launch covers: the launch's colour in a colour-partitioned pass, else all
+static unsigned launch_elements(const nb2_ctx*, const ElementArgs& A) {
+    return (unsigned)A.ecount;
+}
+
 template <int NPE, int MODEL, typename Real, int MODE>
 static void launch_one(nb2_ctx* c, const ElementArgs& A) {
     constexpr int EPC = Topo<NPE>::EPC, G = Topo<NPE>::G;
-    unsigned grid = (unsigned)((c->E + EPC - 1) / EPC);
+    const unsigned grid = (launch_elements(c, A) + EPC - 1) / EPC;
+    if (grid == 0) return;
     k_element<NPE, MODEL, Real, MODE><<<grid, EPC * G, 0, c->stream>>>(A);
     c->launches++;
 }
@@ -1098,11 +1138,14 @@ static int dispatch_model(nb2_ctx* c, const ElementArgs& A, int mode, int precis
 }
 
 static ElementArgs make_args(nb2_ctx* c);
+static bool colour_applies(const nb2_ctx* c, int mode, int precision);
+
 
 template <int NPE>
 static void launch_apply_t(nb2_ctx* c, const ElementArgs& A, const double* v, double* y) {
     constexpr int EPC = Topo<NPE>::EPC, G = Topo<NPE>::G;
-    unsigned grid = (unsigned)((c->E + EPC - 1) / EPC);
+    const unsigned grid = (launch_elements(c, A) + EPC - 1) / EPC;
+    if (grid == 0) return;
     switch (c->mat.model) {
         case MODEL_LE: k_apply<NPE, MODEL_LE><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
         case MODEL_NH: k_apply<NPE, MODEL_NH><<<grid, EPC * G, 0, c->stream>>>(A, v, y); break;
@@ -1119,13 +1162,27 @@ int launch_apply(nb2_ctx* c, const double* v, double* y) {
     int st = upload_tables(c);
     if (st) return st;
     if (!c->dpar || !c->u_tan) return NB2_E_INPUT;
+    bool coloured = false;
+    if (colour_applies(c, MODE_FORCE, NB2_FP64)) {
+        NB2_TRY(ensure_colouring(c));
+        coloured = c->colour_state == 1;
+    }
     ElementArgs A = make_args(c);
     A.u = c->u_tan;
     NB2_CUDA(c, cudaMemsetAsync(y, 0, sizeof(double) * c->n, c->stream));
-    if (c->npe == 8)
+    if (coloured) {
+        // one launch per colour: each node's first term stored, the later colours' added
+        A.ffirst = c->ffirst;
+        for (size_t k = 0; k + 1 < c->h_coff.size(); ++k) {
+            A.order = c->corder + c->h_coff[k];
+            A.ecount = c->h_coff[k + 1] - c->h_coff[k];
+            launch_apply_t<8>(c, A, v, y);
+        }
+    } else if (c->npe == 8) {
         launch_apply_t<8>(c, A, v, y);
-    else
+    } else {
         launch_apply_t<4>(c, A, v, y);
+    }
     NB2_CUDA(c, cudaGetLastError());
     return NB2_OK;
 }
@@ -1273,24 +1330,87 @@ static ElementArgs make_args(nb2_ctx* c) {
     A.e_inst = c->e_inst;
     A.inst_on = c->inst_on;
     A.inst_flags = c->inst_flags;
+    A.order = nullptr;  // colour-partitioned and range passes set these per launch
+    A.ecount = c->E;
+    A.ebegin = 0;
+    A.kfirst = nullptr;
+    A.ffirst = nullptr;
     return A;
+}
+
+// The colour-partitioned scatter (NB2_SCATTER_COLOURED, and always inside nb2_static_solve)
+// serves hex8 passes of one problem that scatter f_int, with the stiffness only in FP64 on the mma
+// path (not the anisotropic microsphere tangent); batched instances (element gating), tet4 and
+// FP32 K keep red.global.add into zeroed arrays.
+static bool colour_applies(const nb2_ctx* c, int mode, int precision) {
+    if (c->scatter != NB2_SCATTER_COLOURED && !c->newton_scatter) return false;
+    if (c->npe != 8 || c->e_inst || !(mode & MODE_FORCE)) return false;
+    if (mode & MODE_STIFFNESS) return precision == NB2_FP64 && !model_aniso(c->mat.model);
+    return true;
 }
 
 int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
     int st = upload_tables(c);
     if (st) return st;
-    const ElementArgs A = make_args(c);
-    if (mode & MODE_STIFFNESS) {
-        if (precision == NB2_FP64)
-            NB2_CUDA(c, cudaMemsetAsync(c->K64, 0, sizeof(double) * 9 * c->nnzb, c->stream));
-        else
-            NB2_CUDA(c, cudaMemsetAsync(c->K32, 0, sizeof(float) * 9 * c->nnzb, c->stream));
+    bool coloured = false;
+    if (colour_applies(c, mode, precision)) {
+        NB2_TRY(ensure_colouring(c));
+        coloured = c->colour_state == 1;
     }
-    if (mode & MODE_FORCE) NB2_CUDA(c, cudaMemsetAsync(c->fint, 0, sizeof(double) * c->n, c->stream));
-    st = (c->npe == 8) ? dispatch_model<8>(c, A, mode, precision)
-                       : dispatch_model<4>(c, A, mode, precision);
-    if (st) return st;
-    // the matrix-free tangent re-derives the gradients from this displacement, not from a
+    ElementArgs A = make_args(c);
+    if (coloured) {
+        // every K block and f_int entry gets its first term stored: no zeroing pass
+        if (mode & MODE_STIFFNESS) A.kfirst = c->kfirst;
+        A.ffirst = c->ffirst;
+        for (size_t k = 0; k + 1 < c->h_coff.size(); ++k) {
+            A.order = c->corder + c->h_coff[k];
+            A.ecount = c->h_coff[k + 1] - c->h_coff[k];
+            st = dispatch_model<8>(c, A, mode, precision);
+            if (st) return st;
+        }
+    } else {
+        if (mode & MODE_FORCE)
+            NB2_CUDA(c, cudaMemsetAsync(c->fint, 0, sizeof(double) * c->n, c->stream));
+        bool ranged = false;
+        if ((mode & MODE_STIFFNESS) && precision == NB2_FP64 && !c->e_inst) {
+            NB2_TRY(ensure_zero_parts(c));
+            ranged = c->zstate == 1;
+        }
+        if (ranged) {
+            // element ranges in order; the K rows range p touches first are zeroed on the second
+            // stream, so zeroing range p+1's rows overlaps range p's element pass
+            const int P = (int)c->zpart_e.size() - 1;
+            NB2_CUDA(c, cudaEventRecord(c->zev[P], c->stream));
+            NB2_CUDA(c, cudaStreamWaitEvent(c->zstream, c->zev[P], 0));
+            for (int p = 0; p < P; ++p) {
+                const long long b0 = c->zpart_b[p], b1 = c->zpart_b[p + 1];
+                if (b1 > b0)
+                    NB2_CUDA(c, cudaMemsetAsync(c->K64 + 9 * b0, 0, sizeof(double) * 9 * (b1 - b0),
+                                                c->zstream));
+                NB2_CUDA(c, cudaEventRecord(c->zev[p], c->zstream));
+            }
+            for (int p = 0; p < P; ++p) {
+                NB2_CUDA(c, cudaStreamWaitEvent(c->stream, c->zev[p], 0));
+                A.ebegin = c->zpart_e[p];
+                A.ecount = c->zpart_e[p + 1] - c->zpart_e[p];
+                st = (c->npe == 8) ? dispatch_model<8>(c, A, mode, precision)
+                                   : dispatch_model<4>(c, A, mode, precision);
+                if (st) return st;
+            }
+        } else {
+            if (mode & MODE_STIFFNESS) {
+                if (precision == NB2_FP64)
+                    NB2_CUDA(c, cudaMemsetAsync(c->K64, 0, sizeof(double) * 9 * c->nnzb,
+                                                c->stream));
+                else
+                    NB2_CUDA(c, cudaMemsetAsync(c->K32, 0, sizeof(float) * 9 * c->nnzb,
+                                                c->stream));
+            }
+            st = (c->npe == 8) ? dispatch_model<8>(c, A, mode, precision)
+                               : dispatch_model<4>(c, A, mode, precision);
+            if (st) return st;
+        }
+    }    // the matrix-free tangent re-derives the gradients from this displacement, not from a
     // later one (the Newton step adds the prescribed increment before its first solve)
     if ((mode & MODE_STORE) && c->u_tan)
         NB2_CUDA(c, cudaMemcpyAsync(c->u_tan, c->u, sizeof(double) * c->n,

@@ -175,6 +175,70 @@ def dirichlet_boundaries(mesh: Mesh, boundaries: list, generate_time_step: float
     return out
 
 
+TRACTION, PRESSURE, BODY_FORCE = 0, 1, 2
+
+
+@dataclasses.dataclass
+class LoadSpec:
+    """One non-follower load boundary (nonfollower_load_boundary, mechanics/solid/boundary/
+    nonfollower_load.cpp:12-121): a traction (component) or a pressure on a group of boundary
+    faces, or a body force (component) over the volume elements, scaled by its time table.
+    Its nodal vector per unit value is computed by whichever implementation solves the problem
+    (the device, or the oracle when it checks the device)."""
+    kind: int
+    times: np.ndarray
+    values: np.ndarray
+    component: int = 0
+    faces: np.ndarray | None = None   # int32 [F, 3 or 4] (surface loads)
+    reduced: bool = False             # quad4 faces on the 1-point rule ("quadrature": "reduced")
+    name: str = ""
+
+
+def nonfollower_loads(mesh: Mesh, boundaries: list, generate_time_step: float = 1.0,
+                      reduced: bool = False) -> list:
+    """The traction / pressure / body_force boundaries of a neon deck as LoadSpecs, in the order
+    neon builds them (nonfollower_load.cpp:21-72: per boundary, traction and body force once per
+    listed component x, y, z; pressure reads its "value" array)."""
+    out = []
+    for b in boundaries:
+        kind = b.get("type", "displacement")
+        if kind not in ("traction", "pressure", "body_force"):
+            continue
+        if kind == "pressure":
+            if "value" not in b:
+                raise ValueError('Pressure boundary condition must specify a "value" array')
+            out.append(LoadSpec(PRESSURE, np.asarray(b["time"], float),
+                                np.asarray(b["value"], float), 0, mesh.faces[b["name"]],
+                                reduced, b["name"]))
+            continue
+        for comp, key in enumerate("xyz"):
+            if key not in b:
+                continue
+            if b.get("generate_type") == "sinusoidal":
+                t, v = sinusoidal_table(b[key][0], b["period"][0], b["number_of_cycles"][0],
+                                        b["phase"][0], generate_time_step)
+            else:
+                t, v = np.asarray(b["time"], float), np.asarray(b[key], float)
+            if kind == "traction":
+                out.append(LoadSpec(TRACTION, t, v, comp, mesh.faces[b["name"]], reduced,
+                                    b["name"]))
+            else:
+                out.append(LoadSpec(BODY_FORCE, t, v, comp, None, False, b["name"]))
+    return out
+
+
+def load_tables(spec: LoadSpec, f: np.ndarray) -> DofTable:
+    """A LoadSpec with its unit-load nodal vector f [3N] as a weighted DOF table."""
+    if spec.kind == BODY_FORCE:
+        nodes = np.arange(len(f) // 3)
+    else:
+        nodes = np.unique(np.asarray(spec.faces).reshape(-1))
+    comps = (0, 1, 2) if spec.kind == PRESSURE else (spec.component,)
+    dofs = np.sort(np.concatenate([3 * nodes + k for k in comps])).astype(np.int32)
+    return DofTable(dofs, np.asarray(spec.times, float), np.asarray(spec.values, float),
+                    weights=f[dofs].copy(), name=spec.name)
+
+
 @dataclasses.dataclass
 class Options:
     """nonlinear_options (static_matrix.hpp:109-143), time/increments
@@ -202,6 +266,7 @@ class Problem:
     options: Options
     nodal_forces: list = dataclasses.field(default_factory=list)
     element_shear_modulus: np.ndarray | None = None
+    loads: list = dataclasses.field(default_factory=list)  # LoadSpec (non-follower loads)
 
     @property
     def ndofs(self) -> int:

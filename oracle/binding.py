@@ -65,6 +65,8 @@ def lib():
         L.orc_get_qp.argtypes = [P, C.c_int, dp]
         L.orc_set_qp.argtypes = [P, C.c_int, dp]
         L.orc_nodal_average.argtypes = [P, C.c_int, dp]
+        L.orc_nonfollower_load.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                           C.c_int, dp]
         L.orc_constitutive_only.argtypes = [P]
         L.orc_cg_solve.argtypes = [C.c_int, ip, ip, dp, dp, dp, C.c_double, C.c_int, C.c_int,
                                    C.POINTER(C.c_int), C.POINTER(C.c_double)]
@@ -202,6 +204,17 @@ class OracleMesh:
         which, _ = QP[name]
         lib().orc_set_qp(self.h, which, np.ascontiguousarray(values, dtype=np.float64).reshape(-1))
 
+    def nonfollower_load(self, kind, component=0, faces=None, reduced=False):
+        """Unit-load nodal vector of a traction / pressure (faces) or a body force (volume),
+        neumann.hpp:69-192 and pressure.cpp:9-37 restated."""
+        f = np.zeros(self.ndofs)
+        fc = None if faces is None else np.ascontiguousarray(faces, dtype=np.int32)
+        nf, npf = (0, 0) if fc is None else fc.shape
+        lib().orc_nonfollower_load(self.h, int(kind), int(component),
+                                   None if fc is None else fc.ctypes.data, int(nf), int(npf),
+                                   int(bool(reduced)), f)
+        return f
+
     def constitutive_only(self):
         return lib().orc_constitutive_only(self.h)
 
@@ -259,12 +272,17 @@ def static_solve(problem, max_log=100000):
                      int(o.adaptive), o.cg_tolerance, o.cg_maximum_iterations, int(o.use_rcm))
     rep = OrcReport()
     bd = _pack_tables(problem.dirichlet)
-    nf = _pack_tables(problem.nodal_forces, weighted=True)
+    # non-follower loads: the oracle forms their nodal vectors itself
+    from neon_b200.problem import load_tables
+    forces = list(problem.nodal_forces) + [
+        load_tables(sp, om.nonfollower_load(sp.kind, sp.component, sp.faces, sp.reduced))
+        for sp in getattr(problem, "loads", [])]
+    nf = _pack_tables(forces, weighted=True)
     u = np.zeros(om.ndofs)
     f = np.zeros(om.ndofs)
     log = np.zeros((max_log, 5))
     lib().orc_static_solve(om.h, C.byref(opt), len(problem.dirichlet), bd[0], bd[1], bd[2], bd[3],
-                           bd[4], len(problem.nodal_forces), nf[0], nf[1], nf[2], nf[3], nf[4],
+                           bd[4], len(forces), nf[0], nf[1], nf[2], nf[3], nf[4],
                            nf[5].ctypes.data if nf[5] is not None else None, u, f, C.byref(rep),
                            log, max_log)
     report = {k: getattr(rep, k) for k, _ in OrcReport._fields_}

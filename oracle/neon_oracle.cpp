@@ -1379,6 +1379,105 @@ struct StaticMatrix {
     }
 };
 
+// Non-follower loads per unit load value (the load's time table scales them), in the initial
+// configuration, accumulated into f [3N] in element order.  Surface groups (quad4 or tri3 faces
+// of the boundary mesh, neon local node order):
+//   traction  f[3a+k] += sum_q w N_a |X,xi x X,eta|            (neumann.hpp:69-133, traction.hpp)
+//   pressure  f[3a+i] += -sum_q w N_a n_i |X,xi x X,eta|, n = (X,xi x X,eta)/|..|
+//             (pressure.cpp:9-37: positive pressure compresses the surface)
+// with quadrilateral4 (interpolations/quadrilateral.cpp:17-45) on the 4-point or, reduced, the
+// 1-point rule (quadrilateral_quadrature.cpp:5-24), triangle3 (interpolations/triangle.cpp:16-40)
+// on its 1-point rule (triangle_quadrature.cpp:12-16, weights x 0.5), chosen as
+// make_surface_interpolation does (interpolation_factory.cpp:99-117).  Volume group (the mesh's
+// own elements):
+//   body force f[3a+k] += sum_q w N_a det(X dN)                (neumann.hpp:135-192, body_force.hpp)
+// kind: 0 traction, 1 pressure, 2 body force; k = component (traction, body force).
+void nonfollower_load(const Oracle& o, int kind, int component, const int* faces, int nfaces,
+                      int npf, int reduced, double* f) {
+    if (kind == 2) {
+        // the volume interpolation: hex8 8-point or tet4 1-point, N at the points
+        const int nq = o.sf.nq, npe = o.npe;
+        std::vector<double> N((size_t)nq * npe);
+        if (npe == 8) {
+            const double lc[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                     {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+            const double g = 1.0 / std::sqrt(3.0);
+            for (int l = 0; l < nq; ++l)
+                for (int a = 0; a < npe; ++a)
+                    N[l * npe + a] = 1.0 / 8.0 * (1.0 + lc[a][0] * lc[l][0] * g) *
+                                     (1.0 + lc[a][1] * lc[l][1] * g) *
+                                     (1.0 + lc[a][2] * lc[l][2] * g);
+        } else {
+            for (int a = 0; a < 4; ++a) N[a] = 0.25;  // (r, s, t, 1-r-s-t) at (1/4, 1/4, 1/4)
+        }
+        for (int e = 0; e < o.E; ++e) {
+            const int* c = &o.conn[(size_t)e * npe];
+            std::vector<double> fe(npe, 0.0);
+            for (int l = 0; l < nq; ++l) {
+                double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                for (int a = 0; a < npe; ++a)
+                    for (int i = 0; i < 3; ++i)
+                        for (int k = 0; k < 3; ++k)
+                            J[i * 3 + k] += o.X[3 * (size_t)c[a] + i] * o.sf.dN[(l * npe + a) * 3 + k];
+                const double j = det3(J);
+                for (int a = 0; a < npe; ++a) fe[a] += N[l * npe + a] * j * o.sf.w[l];
+            }
+            for (int a = 0; a < npe; ++a) f[3 * (size_t)c[a] + component] += fe[a];
+        }
+        return;
+    }
+    // surface interpolation
+    std::vector<double> qxi, qeta, qw;
+    if (npf == 4) {
+        const double g = 1.0 / std::sqrt(3.0);
+        if (reduced) {
+            qxi = {0.0}; qeta = {0.0}; qw = {4.0};
+        } else {
+            qxi = {-g, g, g, -g}; qeta = {-g, -g, g, g}; qw = {1.0, 1.0, 1.0, 1.0};
+        }
+    } else {
+        qxi = {1.0 / 3.0}; qeta = {1.0 / 3.0}; qw = {0.5};
+    }
+    const double lq[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+    for (int fc = 0; fc < nfaces; ++fc) {
+        const int* c = &faces[(size_t)fc * npf];
+        double fe[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (size_t l = 0; l < qw.size(); ++l) {
+            double N[4], r[4][2];
+            if (npf == 4) {
+                for (int a = 0; a < 4; ++a) {
+                    N[a] = 0.25 * (1.0 + lq[a][0] * qxi[l]) * (1.0 + lq[a][1] * qeta[l]);
+                    r[a][0] = 0.25 * (1.0 + lq[a][1] * qeta[l]) * lq[a][0];
+                    r[a][1] = 0.25 * (1.0 + lq[a][0] * qxi[l]) * lq[a][1];
+                }
+            } else {
+                N[0] = qxi[l]; N[1] = qeta[l]; N[2] = 1.0 - qxi[l] - qeta[l];
+                r[0][0] = 1.0; r[0][1] = 0.0; r[1][0] = 0.0; r[1][1] = 1.0;
+                r[2][0] = -1.0; r[2][1] = -1.0;
+            }
+            double t0[3] = {0, 0, 0}, t1[3] = {0, 0, 0};  // the columns of the 3x2 Jacobian
+            for (int a = 0; a < npf; ++a)
+                for (int i = 0; i < 3; ++i) {
+                    t0[i] += o.X[3 * (size_t)c[a] + i] * r[a][0];
+                    t1[i] += o.X[3 * (size_t)c[a] + i] * r[a][1];
+                }
+            const double cr[3] = {t0[1] * t1[2] - t0[2] * t1[1], t0[2] * t1[0] - t0[0] * t1[2],
+                                  t0[0] * t1[1] - t0[1] * t1[0]};
+            const double j = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+            for (int a = 0; a < npf; ++a) {
+                if (kind == 0) {
+                    fe[a][component] += N[a] * j * qw[l];
+                } else {
+                    for (int i = 0; i < 3; ++i) fe[a][i] += N[a] * (cr[i] / j) * j * qw[l];
+                }
+            }
+        }
+        for (int a = 0; a < npf; ++a)
+            for (int i = 0; i < 3; ++i)
+                f[3 * (size_t)c[a] + i] += (kind == 1 ? -fe[a][i] : fe[a][i]);
+    }
+}
+
 }  // namespace
 
 // ========================================================================================
@@ -1717,6 +1816,15 @@ static std::vector<double> extrapolation_matrix(int npe) {
 // each addition counted; the nodal value is the sum over the count.
 // which: 0 Cauchy stress [N][9], 1 det F [N], 2 plastic strain [N][9],
 //        3 accumulated plastic strain [N], 4 von Mises stress [N]
+// unit-load vector of a non-follower load (kind 0 traction, 1 pressure, 2 body force); f [3N]
+// is overwritten
+void orc_nonfollower_load(void* h, int kind, int component, const int* faces, int nfaces, int npf,
+                          int reduced, double* f) {
+    const Oracle& o = *static_cast<Oracle*>(h);
+    std::fill(f, f + o.ndofs(), 0.0);
+    nonfollower_load(o, kind, component, faces, nfaces, npf, reduced, f);
+}
+
 int orc_nodal_average(void* h, int which, double* out) {
     auto* o = static_cast<Oracle*>(h);
     const std::vector<double>* v = nullptr;

@@ -151,6 +151,25 @@ def main(ref: str):
     n_nodes = len(re.findall(r"\[[^\[\]]+\]", coords.group(1))) if coords else 64
     out["cube_fixture"] = {"source": "test/fixtures/cube_mesh.cpp:6-177, test/mesh.cpp:114-267",
                            "nodes": n_nodes, "hex8": n_hex, "active_dofs": 3 * n_nodes}
+    # the fixture's mesh itself: the C++ string literal pieces of json_cube_mesh(), joined and
+    # unescaped, parsed as the .mesh JSON the reference's mesh tests read
+    body = src[src.index("json_cube_mesh()"):]
+    body = body[body.index("return"):body.index(";")]
+    text = "".join(re.findall(r'"((?:[^"\\]|\\.)*)"', body)).replace('\\"', '"')
+    fixture = json.loads(text)
+    with open(os.path.join(HERE, "cube_fixture.json"), "w") as fh:
+        json.dump(fixture, fh, indent=None, separators=(",", ":"))
+    # test/mesh.cpp "Basic mesh test": group sizes, corner coordinates and the unique node lists
+    msrc = open(os.path.join(ref, "test", "mesh.cpp")).read()
+    lists = re.findall(r"known_unique\{([^}]*)\}", msrc)
+    out["cube_fixture_mesh"] = {
+        "source": "test/fixtures/cube_mesh.cpp:6-177 (the mesh, as tests/golden/cube_fixture.json),"
+                  f" test/mesh.cpp:{_find_line(msrc.splitlines(), 'Basic mesh test')}-"
+                  f"{_find_line(msrc.splitlines(), 'Solid submesh test') - 1}",
+        "nodes": 64, "corners": [[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [1.0, 1.0, 0.0]],
+        "elements": {"bottom": 9, "cube": 27, "sides": 36, "top": 9},
+        "unique_nodes": {name: [int(v) for v in re.findall(r"\d+", lst)]
+                         for name, lst in zip(("bottom", "sides", "top"), lists[:3])}}
     # --- neo-Hookean cube example (examples/.../neohooke/cube) ----------------------------
     ex = os.path.join(ref, "examples", "solid_mechanics", "hyperelastic", "neohooke", "cube")
     sim = json.load(open(os.path.join(ex, "cube.json")))

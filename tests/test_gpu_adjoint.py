@@ -120,3 +120,37 @@ def test_langevin_adjoint_matches_central_differences(setup):
         assert abs(grad[e] - fd) <= 1e-5 * abs(fd) + 1e-9 * np.abs(grad).max(), (e, grad[e], fd)
     pr.element_shear_modulus = G0
     assert pr.material.model == P.LANGEVIN_AFFINE_MICROSPHERE
+
+
+def test_c4_full_size_adjoint(setup):
+    """Config 4 at its own size: 48^3 hex8 (110,592 elements), lognormal(0, 0.3) shear-modulus
+    field, top traction; the gradient of J = 1/2 |u_top - u_target|^2 with respect to all
+    110,592 moduli against central differences (h = 1e-4 G_e) on 8 random elements (the
+    configuration asks for 64; each difference is two full forward solves), and the FP32-bulk
+    adjoint against the FP64 one."""
+    api = setup[0]
+    pr = _problem(48, seed=7)
+    assert pr.mesh.num_elements == 110592
+    target = P.config_c4(48, seed_field=99)
+    u_target = api.StaticMatrix(target).solve()
+    sm = api.StaticMatrix(pr)
+    u = sm.solve()
+    _, g = _objective(pr, u, u_target)
+    grad = sm.mesh.adjoint_shear_gradient(g, api.FP64, 1e-13)
+    g32 = sm.mesh.adjoint_shear_gradient(g, api.MIXED, 1e-13)
+    assert rel_err(g32, grad) < 1e-8
+    rng = np.random.Generator(np.random.PCG64(11))
+    G0 = pr.element_shear_modulus.copy()
+    # the elements whose moduli move the top face most, and random ones
+    top_elems = np.argsort(-np.abs(grad))[:4]
+    picks = np.concatenate([top_elems, rng.choice(pr.mesh.num_elements, size=4, replace=False)])
+    for e in picks:
+        h = 1e-4 * G0[e]
+        vals = []
+        for sgn in (1.0, -1.0):
+            pr.element_shear_modulus = G0.copy()
+            pr.element_shear_modulus[e] += sgn * h
+            vals.append(_objective(pr, api.StaticMatrix(pr).solve(), u_target)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(grad[e] - fd) <= 1e-4 * abs(fd) + 1e-6 * np.abs(grad).max(), (e, grad[e], fd)
+    pr.element_shear_modulus = G0

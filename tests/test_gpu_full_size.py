@@ -1,0 +1,147 @@
+"""Parity with the oracle at the benchmark configurations' own sizes, and bit reproducibility of
+the FP64 path.
+
+* C1 (linear elasticity, 20^3 hex8, 27,783 DOFs) in full: the Newton solution with the CG
+  tolerance tightened to 1e-14 on both sides, within 1e-12; K and f_int at that solution within
+  1e-12.
+* C3 (small-strain J2, 100^3 hex8, 3,090,903 DOFs, 245,438,109 nonzeros): K, f_int, the stress
+  and the plastic state after two updates in the plastic range (the state carries over, as in
+  neon's J2 update), all within 1e-12.
+* The FP64 assembly stores every K row and f_int entry once, summed in a fixed order, so two
+  contexts given the same inputs give bit-identical K, f_int, and Newton solutions.
+
+Reference: static_matrix.hpp:243-277 (assembly), :402-467 (Newton), linear_solver.cpp:67-109
+(PCG), small_strain_J2_plasticity.cpp:30-163 (J2 update).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from neon_b200 import problem as P
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def api():
+    from neon_b200 import api, build
+    build.build()
+    api.lib()
+    return api
+
+
+def plastic_displacement(mesh, level=2.5e-3):
+    """Uniaxial z stretch with a shear twist: every point of the J2 cube well past first yield."""
+    X = mesh.X
+    u = np.zeros(3 * mesh.num_nodes)
+    u[2::3] = level * X[:, 2]
+    u[0::3] = 0.3 * level * X[:, 2] * (X[:, 1] - 0.5)
+    u[1::3] = -0.3 * level * X[:, 2] * (X[:, 0] - 0.5)
+    return u
+
+
+def test_c1_full_size_solution_and_system(api, oracle):
+    pr = P.config_c1(20)
+    assert pr.ndofs == 27783
+    pr.options.cg_tolerance = 1e-14
+    pr.options.cg_maximum_iterations = 200000
+    rep_o, u_o, _, log_o, _ = oracle.static_solve(pr)
+    assert rep_o["status"] == 0, rep_o["message"]
+    sm = api.StaticMatrix(pr)
+    u = sm.solve()
+    assert sm.report["newton_iterations"] == rep_o["newton_iterations"]
+    assert np.array_equal(sm.log[:, :2], log_o[:, :2])
+    assert rel_err(u, u_o) < TOL
+    g = api.SolidMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+    om = oracle.OracleMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+    assert g.nnz == om.nnz == 2042829
+    g.update_internal_variables(u_o)
+    assert om.update(u_o)[0] == 0
+    K, f = g.assemble()
+    assert rel_err(K, om.assemble()) < TOL
+    assert rel_err(f, om.internal_force()) < TOL
+
+
+def test_c3_full_size_assembly_and_state(api, oracle):
+    pr = P.config_c3(100)
+    g = api.SolidMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+    om = oracle.OracleMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+    assert g.ndofs == 3090903 and g.nnz == om.nnz == 245438109
+    u = plastic_displacement(pr.mesh)
+    for scale in (0.5, 1.0):  # two updates: neon's J2 state carries over between calls
+        st, msg = om.update(scale * u)
+        assert st == 0, msg
+        g.update_internal_variables(scale * u)
+    assert om.get("epbar").min() > 0.0  # every point has yielded
+    K, f = g.assemble()
+    assert rel_err(K, om.assemble()) < TOL
+    del K
+    assert rel_err(f, om.internal_force()) < TOL
+    assert rel_err(g.quadrature_values("cauchy_stress"), om.get("sigma")) < TOL
+    assert rel_err(g.quadrature_values("plastic_strain"), om.get("ep")) < TOL
+    assert rel_err(g.quadrature_values("accumulated_plastic_strain"), om.get("epbar")) < TOL
+
+
+def test_fp64_assembly_is_bit_reproducible(api):
+    """Two contexts with the coloured scatter, same inputs: identical K, f_int, state and
+    matrix-free product, bit for bit; the red-based scatter gives the same values to rounding."""
+    pr = P.config_c3(40)
+    u = plastic_displacement(pr.mesh)
+    out = []
+    for mode in (api.SCATTER_COLOURED, api.SCATTER_COLOURED, api.SCATTER_RED):
+        g = api.SolidMesh(pr.mesh.X, pr.mesh.conn, pr.material)
+        g.set_scatter_mode(mode)
+        g.update_internal_variables(0.5 * u)
+        g.update_internal_variables(u)
+        K, f = g.assemble()
+        y = g.apply_tangent(np.sin(np.arange(g.ndofs, dtype=np.float64)))
+        out.append((K, f, g.quadrature_values("accumulated_plastic_strain"), y))
+        g.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+    for a, b in zip(out[0], out[2]):
+        assert rel_err(a, b) < 1e-14
+
+
+def test_fp64_newton_is_bit_reproducible(api):
+    """The FP64 Newton path with J2 in the plastic range (where a last-bit change of K moves the
+    converged displacement by ~1e-6 through neon's path-dependent update) gives the same
+    displacement, bit for bit, when run twice; so does the mixed-precision path."""
+    pr = P.config_c3(16, steps=20)
+    pr.options.period = 5.0  # the first quarter cycle: the top face loads into the plastic range
+    u1 = api.StaticMatrix(pr).solve()
+    u2 = api.StaticMatrix(pr).solve()
+    assert np.array_equal(u1, u2)
+    m1 = api.StaticMatrix(pr, precision=api.MIXED, mixed_inner_tolerance=1e-3).solve()
+    m2 = api.StaticMatrix(pr, precision=api.MIXED, mixed_inner_tolerance=1e-3).solve()
+    assert np.array_equal(m1, m2)
+
+
+def _newton_parity(api, oracle, pr):
+    rep_o, u_o, _, log_o, _ = oracle.static_solve(pr)
+    assert rep_o["status"] == 0, rep_o["message"]
+    sm = api.StaticMatrix(pr)
+    u = sm.solve()
+    assert sm.report["status"] == 0, sm.report["message"]
+    assert sm.report["newton_iterations"] == rep_o["newton_iterations"]
+    assert np.array_equal(sm.log[:, :2], log_o[:, :2])
+    return rel_err(u, u_o)
+
+
+def test_c2_full_size_first_increment(api, oracle):
+    """Neo-Hooke on the jittered 64^3 mesh (823,875 DOFs), the first of the ten increments:
+    several Newton iterations at CG rtol 1e-10 leave the two solutions within 1e-12."""
+    pr = P.config_c2(64)
+    assert pr.ndofs == 823875
+    pr.options.period = pr.options.initial  # the first increment only
+    assert _newton_parity(api, oracle, pr) < TOL
+
+
+def test_c4_full_size_forward_solve(api, oracle):
+    """Gaussian affine microsphere on 48^3 (352,947 DOFs) with the lognormal shear-modulus field
+    and the top traction: the forward solve the adjoint gradient is taken at."""
+    pr = P.config_c4(48)
+    assert pr.ndofs == 352947
+    assert _newton_parity(api, oracle, pr) < TOL

@@ -351,3 +351,55 @@ def test_uniaxial_patch_neo_hooke_jittered(oracle):
     # sigma_xx = 0: lam ln J + mu (l^2 - 1) = 0 with J = s l^2
     l = brentq(lambda l: lam * np.log(s * l * l) + mu * (l * l - 1.0), 0.5, 1.0)
     np.testing.assert_allclose(u[0::3], (l - 1.0) * X[:, 0], atol=1e-8)
+
+
+def _triangle_mesh(oracle):
+    """The reference's right triangle (0,0,0), (1,0,0), (0,1,0) as face 0-1-2 of a tet4."""
+    X = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+    mat = P.make_material({"elastic_modulus": 1.0, "poissons_ratio": 0.3},
+                          {"name": "isotropic_linear_elasticity"})
+    return oracle.OracleMesh(X, np.array([[0, 1, 2, 3]], np.int32), mat)
+
+
+def test_triangle_traction_and_pressure_known_answers(oracle):
+    """test/boundary.cpp:72-112 (traction 1 on the triangle: 1/6 per node, 2 -> 2/6) and
+    :114-166 (pressure -1: z components 1/6, -2 -> 2/6)."""
+    om = _triangle_mesh(oracle)
+    tri = np.array([[0, 1, 2]], np.int32)
+    t = om.nonfollower_load(P.TRACTION, 0, tri)
+    np.testing.assert_allclose(t[[0, 3, 6]], 1.0 / 6.0, atol=1e-15)
+    np.testing.assert_allclose(2.0 * t[[0, 3, 6]], 2.0 / 6.0, atol=1e-15)
+    assert np.count_nonzero(t) == 3
+    p = om.nonfollower_load(P.PRESSURE, 0, tri)
+    np.testing.assert_allclose(-1.0 * p[[2, 5, 8]], 1.0 / 6.0, atol=1e-15)
+    np.testing.assert_allclose(-2.0 * p[[2, 5, 8]], 2.0 / 6.0, atol=1e-15)
+    np.testing.assert_allclose(p[[0, 1, 3, 4, 6, 7, 9, 10, 11]], 0.0, atol=1e-15)
+
+
+def test_nonfollower_load_integrals(oracle):
+    """Consistent loads integrate exactly: the traction vector sums to the face area, the body
+    force to the volume, and a pressure on a closed surface to zero (divergence theorem), on a
+    cube whose boundary is warped so the faces are not planar."""
+    m = M.structured_hex8(4, 3, 5)
+    X = m.X.copy()
+    X += 0.03 * np.sin(np.pi * X[:, [1, 2, 0]]) * np.sin(np.pi * X[:, [2, 0, 1]])
+    mat = P.make_material({"elastic_modulus": 1.0, "poissons_ratio": 0.3},
+                          {"name": "isotropic_linear_elasticity"})
+    om = oracle.OracleMesh(X, m.conn, mat)
+    closed = np.concatenate([m.faces[k] for k in ("bottom", "top", "x0", "x1", "y0", "y1")])
+    p = om.nonfollower_load(P.PRESSURE, 0, closed).reshape(-1, 3)
+    assert np.abs(p.sum(axis=0)).max() < 1e-13
+    # volume: det J summed over the 8-point rule (exact for trilinear maps)
+    b = om.nonfollower_load(P.BODY_FORCE, 2, None)
+    q = om.nonfollower_load(P.BODY_FORCE, 0, None)
+    assert abs(b.sum() - q.sum()) < 1e-14 and b.sum() > 0.9
+    top = m.faces["top"]
+    t = om.nonfollower_load(P.TRACTION, 2, top)
+    tr = om.nonfollower_load(P.TRACTION, 2, top, reduced=True)
+    assert abs(t.sum() - tr.sum()) < 0.05 * t.sum()  # 1-point vs 4-point area of a warped face
+    # a flat face (the structured mesh): the area is exact on both rules
+    om0 = oracle.OracleMesh(m.X, m.conn, mat)
+    a4 = om0.nonfollower_load(P.TRACTION, 2, top).sum()
+    a1 = om0.nonfollower_load(P.TRACTION, 2, top, reduced=True).sum()
+    assert abs(a4 - 1.0) < 1e-14 and abs(a1 - 1.0) < 1e-14
+    assert abs(om0.nonfollower_load(P.BODY_FORCE, 1, None).sum() - 1.0) < 1e-14
