@@ -339,6 +339,8 @@ def main():
     ap.add_argument("--newton-load-steps", type=int, default=2)
     ap.add_argument("--newton-cyclic-increments", type=int, default=24,
                     help="increments of the cyclic segment (80 = the whole 20-step cycle)")
+    ap.add_argument("--newton-cyclic-sensitivity", action="store_true",
+                    help="also run the cyclic segment in FP64 at rtol 1e-11")
     ap.add_argument("--no-newton", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -347,6 +349,7 @@ def main():
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-c2", action="store_true")
     ap.add_argument("--adjoint-size", type=int, default=48)
     ap.add_argument("--cpu-newton", action="store_true",
                     help="only time the oracle's Newton steps (C1, C2, C3) and print them")
@@ -484,6 +487,10 @@ def main():
         newton = newton_comparison(api, P, args, mesh)
 
     log("newton done")
+    c2 = c1 = None
+    if not args.no_newton and not args.no_c2:
+        c2 = c2_newton(api, P)
+        c1 = c2_newton(api, P, "c1")
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_timing(api, P, args)
@@ -508,7 +515,7 @@ def main():
             "coloured_scatter": coloured, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "timed_region_ms": region_ms, "clocks": clock_info,
             "fp32_fma_peak_tflops": fp32_peak / 1e12, "pcg": pcg, "newton": newton,
-            "adjoint": adjoint, "batched": batched}
+            "c1_newton": c1, "c2_newton": c2, "adjoint": adjoint, "batched": batched}
     if rank == 0:
         print(json.dumps(line), flush=True)
     mesh.close()
@@ -649,12 +656,43 @@ def newton_comparison(api, P, args, mesh_unused):
                 "fp64": q64, "mixed": q32, "mixed_rel_err_u": _rel(t32, t64),
                 "newton_step_speedup": q64["newton_step_s"] / max(q32["newton_step_s"], 1e-12)}
             log(f"newton {name} rtol 1e-12: mixed err {seg['rtol_1e-12']['mixed_rel_err_u']:.2e}")
+        if name == "cyclic" and args.newton_cyclic_sensitivity:
+            # the FP64 path against itself at rtol 1e-11 over the same cycle segment
+            u64b, _ = _newton_run(api, P, args.size, steps, api.FP64, cg_tol=1e-11)
+            seg["fp64_rtol_sensitivity_rel_err_u"] = _rel(u64b, u64)
+            log(f"newton {name} fp64 rtol sensitivity {seg['fp64_rtol_sensitivity_rel_err_u']:.2e}")
         out["segments"][name] = seg
     main = out["segments"]["cyclic" if "cyclic" in out["segments"] else "yielding"]
     out["newton_step_s_fp64"] = main["fp64"]["newton_step_s"]
     out["newton_step_s_mixed"] = main["mixed"]["newton_step_s"]
     out["newton_step_speedup"] = main["newton_step_speedup"]
     out["mixed_rel_err_u"] = main["mixed_rel_err_u"]
+    return out
+
+
+def c2_newton(api, P, config="c2"):
+    """Config 2 in full (neo-Hooke, jittered 64^3 hex8, 823,875 DOFs, stretch to 1.3 in 10
+    increments), or config 1 in full (linear elasticity, 20^3, one increment): FP64 and mixed
+    device Newton, seconds per Newton step and the relative difference of the final
+    displacements (neither model is path dependent)."""
+    out = {}
+    us = {}
+    for name, prec in (("fp64", api.FP64), ("mixed", api.MIXED)):
+        pr = P.config_c2(64) if config == "c2" else P.config_c1(20)
+        sm = api.StaticMatrix(pr, precision=prec, mixed_inner_tolerance=1e-3)
+        try:
+            us[name] = sm.solve(raise_on_error=False)
+        finally:
+            sm.mesh.close()
+        r = sm.report
+        nit = max(1, int(r["newton_iterations"]))
+        out[name] = {"status": int(r["status"]), "load_steps": int(r["load_steps"]),
+                     "newton_iterations": nit, "cg_iterations": int(r["cg_iterations"]),
+                     "seconds_total": r["seconds_total"], "newton_step_s": r["seconds_total"] / nit}
+        log(f"{config} {name}: {r['seconds_total']:.2f} s")
+    out["mixed_rel_err_u"] = _rel(us["mixed"], us["fp64"])
+    out["newton_step_speedup"] = out["fp64"]["newton_step_s"] / max(out["mixed"]["newton_step_s"],
+                                                                   1e-12)
     return out
 
 

@@ -162,16 +162,16 @@ int nb2_set_stream(nb2_ctx* ctx, void* stream);
  * counterpart: neon adds with OpenMP atomics (thread_safe_plugin.hpp:7-23), so its sums run in
  * a thread-dependent order.
  *   NB2_SCATTER_RED       (default for nb2_update_internal_variables / nb2_assemble /
- *                         nb2_update_assemble_device) red.global.add into zeroed arrays: the
- *                         fastest; the order of the additions, and so the last bits, can
- *                         change from run to run.
- *   NB2_SCATTER_COLOURED  one launch per element colour (elements of a colour share no node):
- *                         every entry's first term is stored and the later colours' terms added,
- *                         in colour order, so the same inputs give bit-identical K and f_int.
- * nb2_static_solve always uses the coloured scatter, whatever this setting: its Newton iterates,
- * CG and solution are then bit-reproducible (the element passes are ~1% of a Newton step).
- * tet4 meshes, the anisotropic microsphere tangent, FP32 K and batched instances always use
- * red.global.add. */
+ *                         nb2_update_assemble_device) every element in one launch, terms added
+ *                         with red.global.add into zeroed arrays: the fastest; the order of the
+ *                         additions, and so the last bits, can change from run to run.
+ *   NB2_SCATTER_COLOURED  one launch per element colour (elements of a colour share no node),
+ *                         so an entry receives at most one addition per launch and its sum runs
+ *                         in colour order: the same inputs give bit-identical K and f_int.
+ * nb2_static_solve always uses the coloured launches, whatever this setting: its Newton
+ * iterates, CG and solution are then bit-reproducible (the element passes are ~1% of a Newton
+ * step).  tet4 meshes, the anisotropic microsphere tangent, FP32 K and batched instances always
+ * use one launch. */
 #define NB2_SCATTER_RED 0
 #define NB2_SCATTER_COLOURED 1
 int nb2_set_scatter_mode(nb2_ctx* ctx, int32_t mode);

@@ -211,7 +211,11 @@ class SolidMesh:
             self.h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter exit the module globals (lib, _lib) may already be gone
+        try:
+            self.close()
+        except (TypeError, AttributeError):
+            pass
 
     # --- neon mesh / submesh API -----------------------------------------------------------
     def sparsity_pattern(self):

@@ -228,12 +228,9 @@ int nb2_destroy(nb2_ctx* c) {
                     c->ep_old, c->epbar_old, c->sig, c->dpar,   c->detF,      c->cg_x,
                     c->cg_r,   c->cg_p,   c->cg_q,   c->cg_inv, c->cg32_x,    c->cg32_r,
                     c->cg32_p, c->cg32_q, c->cg32_inv, c->partials, c->cgs,   c->norms,
-                    c->status, c->corder, c->kfirst, c->ffirst};
+                    c->status, c->corder};
     for (void* p : ptrs)
         if (p) cudaFree(p);
-    for (cudaEvent_t ev : c->zev)
-        if (ev) cudaEventDestroy(ev);
-    if (c->zstream) cudaStreamDestroy(c->zstream);
     if (c->h_cgs) cudaFreeHost(c->h_cgs);
     if (c->h_norms) cudaFreeHost(c->h_norms);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);

@@ -8,11 +8,10 @@
 //            reduce-scatter, so lane l ends with node l's force);
 //   phase 2  hex8 in FP64 (every model but the anisotropic microspheres): each warp forms the
 //            64 blocks of its elements, one element at a time, as 8x8 node x node tiles with
-//            FP64 mma.sync, stages them in shared memory and writes them to K, consecutive
-//            lanes on consecutive entries of a block: in a colour-partitioned pass (A.order) a
-//            block's first term is stored and the later colours' terms added, so no entry ever
-//            has two writers at once and the sums run in colour order; otherwise each term is
-//            added with red.global.add into a zeroed K;
+//            FP64 mma.sync, stages them in shared memory and adds them to K with red.global.add,
+//            consecutive lanes on consecutive entries of a block (in a colour-partitioned pass,
+//            A.order, an entry gets at most one term per launch, so the sums run in colour
+//            order);
 //            otherwise: each lane accumulates its upper-triangular 3x3 blocks over the points in
 //            Real precision, in passes of at most 3 blocks (fewer live registers), and adds them
 //            (and their mirrored blocks) to K with red.global.add.
@@ -308,21 +307,13 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
 
     if constexpr (kForce) {
         if (valid) {
-            const unsigned fm = A.ffirst ? A.ffirst[e] : 0u;
 #pragma unroll
             for (int j = 0; j < NG; ++j) {
                 const int a = lane + j * G;
                 if (a < NPE) {
-                    double* fa = &A.fint[3ll * node[j]];
-                    if ((fm >> a) & 1u) {  // this node's first term in colour order
-                        fa[0] = fown[j][0];
-                        fa[1] = fown[j][1];
-                        fa[2] = fown[j][2];
-                    } else {
-                        atomicAdd(&fa[0], fown[j][0]);
-                        atomicAdd(&fa[1], fown[j][1]);
-                        atomicAdd(&fa[2], fown[j][2]);
-                    }
+                    atomicAdd(&A.fint[3ll * node[j] + 0], fown[j][0]);
+                    atomicAdd(&A.fint[3ll * node[j] + 1], fown[j][1]);
+                    atomicAdd(&A.fint[3ll * node[j] + 2], fown[j][2]);
                 }
             }
         }
@@ -348,7 +339,6 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
             if (!element_enabled(A, e2)) continue;  // the same for all lanes of the warp
             const int* slot = A.slot + e2 * (NPE * NPE);
             const int sl0 = slot[lane32], sl1 = slot[32 + lane32];
-            const unsigned long long kf = A.kfirst ? A.kfirst[e2] : 0ull;
             double Lq[2][3], cl[2], cm[2], cb[2];
 #pragma unroll
             for (int st = 0; st < 2; ++st) {
@@ -434,12 +424,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                 const int idx = it * 32 + lane32;
                 const int blk = idx / 9;
                 const long long sab = sSl[warp][blk];
-                const double v = sKe[warp][idx + (blk >> 4)];
-                double* kp = &Kp[9 * sab + (idx - 9 * blk)];
-                if ((kf >> blk) & 1ull)  // the block's first term in colour order
-                    *kp = v;
-                else
-                    atomicAdd(kp, v);
+                atomicAdd(&Kp[9 * sab + (idx - 9 * blk)], sKe[warp][idx + (blk >> 4)]);
             }
             __syncwarp();
         }

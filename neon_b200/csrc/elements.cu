@@ -525,7 +525,7 @@ __device__ __forceinline__ bool element_enabled(const ElementArgs& A, long long 
 // colour-partitioned pass, else element pos; -1 past the end
 __device__ __forceinline__ long long element_at(const ElementArgs& A, long long pos) {
     if (pos >= A.ecount) return -1;
-    return A.order ? (long long)A.order[pos] : A.ebegin + pos;
+    return A.order ? (long long)A.order[pos] : pos;
 }
 
 // D += A B for one 8x8x4 FP64 tile (mma.sync m8n8k4, row.col): lane l holds A[l/4][l%4],
@@ -668,7 +668,6 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
     }
     __syncthreads();
     if (!valid) return;
-    const unsigned fm = A.ffirst ? A.ffirst[e] : 0u;
 #pragma unroll
     for (int j = 0; j < (NPE + G - 1) / G; ++j) {
         int a = lane + j * G;
@@ -680,16 +679,9 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
                 f1 += sY[le][l][3 * a + 1];
                 f2 += sY[le][l][3 * a + 2];
             }
-            double* ya = &y[3ll * node[j]];
-            if ((fm >> a) & 1u) {  // first term of this node in colour order
-                ya[0] = f0;
-                ya[1] = f1;
-                ya[2] = f2;
-            } else {
-                atomicAdd(&ya[0], f0);
-                atomicAdd(&ya[1], f1);
-                atomicAdd(&ya[2], f2);
-            }
+            atomicAdd(&y[3ll * node[j] + 0], f0);
+            atomicAdd(&y[3ll * node[j] + 1], f1);
+            atomicAdd(&y[3ll * node[j] + 2], f2);
         }
     }
 }
@@ -1171,8 +1163,7 @@ int launch_apply(nb2_ctx* c, const double* v, double* y) {
     A.u = c->u_tan;
     NB2_CUDA(c, cudaMemsetAsync(y, 0, sizeof(double) * c->n, c->stream));
     if (coloured) {
-        // one launch per colour: each node's first term stored, the later colours' added
-        A.ffirst = c->ffirst;
+        // one launch per colour: each entry gets at most one term per launch, in colour order
         for (size_t k = 0; k + 1 < c->h_coff.size(); ++k) {
             A.order = c->corder + c->h_coff[k];
             A.ecount = c->h_coff[k + 1] - c->h_coff[k];
@@ -1330,18 +1321,15 @@ static ElementArgs make_args(nb2_ctx* c) {
     A.e_inst = c->e_inst;
     A.inst_on = c->inst_on;
     A.inst_flags = c->inst_flags;
-    A.order = nullptr;  // colour-partitioned and range passes set these per launch
+    A.order = nullptr;  // colour-partitioned passes set these per launch
     A.ecount = c->E;
-    A.ebegin = 0;
-    A.kfirst = nullptr;
-    A.ffirst = nullptr;
     return A;
 }
 
-// The colour-partitioned scatter (NB2_SCATTER_COLOURED, and always inside nb2_static_solve)
-// serves hex8 passes of one problem that scatter f_int, with the stiffness only in FP64 on the mma
+// The colour-partitioned launches (NB2_SCATTER_COLOURED, and always inside nb2_static_solve)
+// serve hex8 passes of one problem that scatter f_int, with the stiffness only in FP64 on the mma
 // path (not the anisotropic microsphere tangent); batched instances (element gating), tet4 and
-// FP32 K keep red.global.add into zeroed arrays.
+// FP32 K use one launch.
 static bool colour_applies(const nb2_ctx* c, int mode, int precision) {
     if (c->scatter != NB2_SCATTER_COLOURED && !c->newton_scatter) return false;
     if (c->npe != 8 || c->e_inst || !(mode & MODE_FORCE)) return false;
@@ -1358,10 +1346,16 @@ int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
         coloured = c->colour_state == 1;
     }
     ElementArgs A = make_args(c);
+    if (mode & MODE_STIFFNESS) {
+        if (precision == NB2_FP64)
+            NB2_CUDA(c, cudaMemsetAsync(c->K64, 0, sizeof(double) * 9 * c->nnzb, c->stream));
+        else
+            NB2_CUDA(c, cudaMemsetAsync(c->K32, 0, sizeof(float) * 9 * c->nnzb, c->stream));
+    }
+    if (mode & MODE_FORCE) NB2_CUDA(c, cudaMemsetAsync(c->fint, 0, sizeof(double) * c->n, c->stream));
     if (coloured) {
-        // every K block and f_int entry gets its first term stored: no zeroing pass
-        if (mode & MODE_STIFFNESS) A.kfirst = c->kfirst;
-        A.ffirst = c->ffirst;
+        // one launch per colour: an entry of K or f_int receives at most one term per launch,
+        // so its additions arrive in colour order on every run
         for (size_t k = 0; k + 1 < c->h_coff.size(); ++k) {
             A.order = c->corder + c->h_coff[k];
             A.ecount = c->h_coff[k + 1] - c->h_coff[k];
@@ -1369,48 +1363,11 @@ int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
             if (st) return st;
         }
     } else {
-        if (mode & MODE_FORCE)
-            NB2_CUDA(c, cudaMemsetAsync(c->fint, 0, sizeof(double) * c->n, c->stream));
-        bool ranged = false;
-        if ((mode & MODE_STIFFNESS) && precision == NB2_FP64 && !c->e_inst) {
-            NB2_TRY(ensure_zero_parts(c));
-            ranged = c->zstate == 1;
-        }
-        if (ranged) {
-            // element ranges in order; the K rows range p touches first are zeroed on the second
-            // stream, so zeroing range p+1's rows overlaps range p's element pass
-            const int P = (int)c->zpart_e.size() - 1;
-            NB2_CUDA(c, cudaEventRecord(c->zev[P], c->stream));
-            NB2_CUDA(c, cudaStreamWaitEvent(c->zstream, c->zev[P], 0));
-            for (int p = 0; p < P; ++p) {
-                const long long b0 = c->zpart_b[p], b1 = c->zpart_b[p + 1];
-                if (b1 > b0)
-                    NB2_CUDA(c, cudaMemsetAsync(c->K64 + 9 * b0, 0, sizeof(double) * 9 * (b1 - b0),
-                                                c->zstream));
-                NB2_CUDA(c, cudaEventRecord(c->zev[p], c->zstream));
-            }
-            for (int p = 0; p < P; ++p) {
-                NB2_CUDA(c, cudaStreamWaitEvent(c->stream, c->zev[p], 0));
-                A.ebegin = c->zpart_e[p];
-                A.ecount = c->zpart_e[p + 1] - c->zpart_e[p];
-                st = (c->npe == 8) ? dispatch_model<8>(c, A, mode, precision)
-                                   : dispatch_model<4>(c, A, mode, precision);
-                if (st) return st;
-            }
-        } else {
-            if (mode & MODE_STIFFNESS) {
-                if (precision == NB2_FP64)
-                    NB2_CUDA(c, cudaMemsetAsync(c->K64, 0, sizeof(double) * 9 * c->nnzb,
-                                                c->stream));
-                else
-                    NB2_CUDA(c, cudaMemsetAsync(c->K32, 0, sizeof(float) * 9 * c->nnzb,
-                                                c->stream));
-            }
-            st = (c->npe == 8) ? dispatch_model<8>(c, A, mode, precision)
-                               : dispatch_model<4>(c, A, mode, precision);
-            if (st) return st;
-        }
-    }    // the matrix-free tangent re-derives the gradients from this displacement, not from a
+        st = (c->npe == 8) ? dispatch_model<8>(c, A, mode, precision)
+                           : dispatch_model<4>(c, A, mode, precision);
+        if (st) return st;
+    }
+    // the matrix-free tangent re-derives the gradients from this displacement, not from a
     // later one (the Newton step adds the prescribed increment before its first solve)
     if ((mode & MODE_STORE) && c->u_tan)
         NB2_CUDA(c, cudaMemcpyAsync(c->u_tan, c->u, sizeof(double) * c->n,

@@ -85,15 +85,12 @@ struct ElementArgs {
     const int* e_inst;
     const int* inst_on;
     unsigned int* inst_flags;
-    // colour-partitioned scatter (null: red.global.add into zeroed K / f_int).  A pass runs one
+    // colour-partitioned launches (null: all elements in one launch).  A pass then runs one
     // launch per element colour; elements of one colour share no node, so every K entry and
-    // f_int entry receives at most one contribution per launch, in colour order: the first
-    // contribution is stored, the later ones added (deterministic, no zeroing pass).
+    // f_int entry receives at most one red.global.add per launch and its sum runs in colour
+    // order: the same inputs give the same bits on every run.
     const int* order;                  // element indices of this launch's colour
-    int ecount;                        // elements of this launch (its colour, or its range)
-    int ebegin;                        // first element of a range launch (order == null)
-    const unsigned long long* kfirst;  // [E] bit b: element block b is its K block's first term
-    const unsigned char* ffirst;       // [E] bit a: the element is node a's first f_int term
+    int ecount;                        // elements of this launch
 };
 
 // PCG scalars kept on the device (no host round trip per iteration)
@@ -159,23 +156,12 @@ struct nb2_ctx {
     float* mf_ye = nullptr;  // [E][npe*3]
     int* nadj_ptr = nullptr; // [N+1]
     int* nadj = nullptr;     // [E*npe] element slots e*npe + a, grouped by node
-    // colour-partitioned scatter (hex8, single problem): elements grouped by colour, first-term
-    // masks of the K blocks and f_int entries
+    // colour-partitioned launches (hex8, single problem): elements grouped by colour
     int* corder = nullptr;                   // [E] elements sorted by colour
     std::vector<int> h_coff;                 // colour offsets into corder
-    unsigned long long* kfirst = nullptr;    // [E]
-    unsigned char* ffirst = nullptr;         // [E]
     int colour_state = 0;  // 0 not set up, 1 ready, -1 not applicable (tet4, > 64 colours)
-    int scatter = NB2_SCATTER_RED;  // element-pass scatter mode (nb2_set_scatter_mode)
-    // red-based FP64 passes in element ranges: K rows a range touches first are zeroed on a
-    // second stream while the previous range runs (zparts + 1 element offsets, BSR block offsets
-    // of the rows each range zeroes; empty when the ranges' rows are not contiguous)
-    std::vector<int> zpart_e;
-    std::vector<long long> zpart_b;
-    cudaStream_t zstream = nullptr;
-    cudaEvent_t zev[8] = {};
-    int zstate = 0;  // 0 not set up, 1 ready, -1 not applicable
-    bool newton_scatter = false;    // set while nb2_static_solve runs: coloured scatter
+    int scatter = NB2_SCATTER_RED;  // element-pass launch mode (nb2_set_scatter_mode)
+    bool newton_scatter = false;    // set while nb2_static_solve runs: colour-partitioned
     cudaGraphExec_t graph_mf = nullptr;
 
     // PCG workspace (FP64 and FP32 views share nothing)
@@ -232,8 +218,7 @@ int read_status(nb2_ctx* c);           // synchronises; the status code + neon's
 // pattern.cu
 int build_pattern(nb2_ctx* c);
 int build_node_adjacency(nb2_ctx* c);  // nadj_ptr / nadj
-int ensure_colouring(nb2_ctx* c);      // element colours + first-term masks (hex8)
-int ensure_zero_parts(nb2_ctx* c);     // element ranges whose first-touched K rows are contiguous
+int ensure_colouring(nb2_ctx* c);      // element colours and the colour-sorted element list
 int export_csr_values(nb2_ctx* c, const double* Kbsr, double* Kcsr_dev);
 
 // elements.cu

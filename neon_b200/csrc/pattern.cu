@@ -162,43 +162,10 @@ int build_node_adjacency(nb2_ctx* c) {
     return NB2_OK;
 }
 
-// first colour to reach each K block and each node (atomicMin: order-independent)
-__global__ void k_first_colour(long long m, int npe, const int* __restrict__ slot,
-                               const int* __restrict__ conn, const unsigned char* __restrict__ col,
-                               int* __restrict__ fblock, int* __restrict__ fnode) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= m) return;
-    const long long e = t / (npe * npe);
-    const int cl = col[e];
-    atomicMin(&fblock[slot[t]], cl);
-    const int ab = (int)(t % (npe * npe));
-    if (ab % (npe + 1) == 0) atomicMin(&fnode[conn[e * npe + ab / (npe + 1)]], cl);
-}
-
-// per element: which of its blocks and nodes receive their first term from it
-__global__ void k_first_masks(int E, int npe, const int* __restrict__ slot,
-                              const int* __restrict__ conn, const unsigned char* __restrict__ col,
-                              const int* __restrict__ fblock, const int* __restrict__ fnode,
-                              unsigned long long* __restrict__ kfirst,
-                              unsigned char* __restrict__ ffirst) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= E) return;
-    const int cl = col[e];
-    unsigned long long km = 0ull;
-    unsigned fm = 0u;
-    for (int b = 0; b < npe * npe; ++b)
-        if (fblock[slot[(long long)e * npe * npe + b]] == cl) km |= 1ull << b;
-    for (int a = 0; a < npe; ++a)
-        if (fnode[conn[(long long)e * npe + a]] == cl) fm |= 1u << a;
-    kfirst[e] = km;
-    ffirst[e] = (unsigned char)fm;
-}
-
-// Element colouring for the colour-partitioned scatter (hex8, one problem).  Greedy first fit in
+// Element colouring for the colour-partitioned launches (hex8, one problem).  Greedy first fit in
 // element order over the node-sharing graph (a structured hex8 mesh gets the 8 parity colours);
-// the elements are then grouped by colour, and each element gets the mask of the K blocks and
-// nodes whose first contribution (in colour order) is its own.  Not applicable (colour_state -1)
-// to tet4 or when more than 64 colours would be needed.
+// the elements are then listed colour by colour.  Not applicable (colour_state -1) to tet4 or
+// when more than 64 colours would be needed.
 int ensure_colouring(nb2_ctx* c) {
     if (c->colour_state != 0) return NB2_OK;
     if (c->npe != 8) {
@@ -240,81 +207,12 @@ int ensure_colouring(nb2_ctx* c) {
     for (int k = 0; k < ncol; ++k) coff[k + 1] += coff[k];
     std::vector<int> pos(coff.begin(), coff.end() - 1);
     for (int e = 0; e < E; ++e) order[pos[col[e]]++] = e;
-    unsigned char* dcol = nullptr;
-    int *fblock = nullptr, *fnode = nullptr;
     NB2_CUDA(c, cudaMalloc(&c->corder, sizeof(int) * E));
-    NB2_CUDA(c, cudaMalloc(&c->kfirst, sizeof(unsigned long long) * E));
-    NB2_CUDA(c, cudaMalloc(&c->ffirst, E));
-    NB2_CUDA(c, cudaMallocAsync(&dcol, E, c->stream));
-    NB2_CUDA(c, cudaMallocAsync(&fblock, sizeof(int) * c->nnzb, c->stream));
-    NB2_CUDA(c, cudaMallocAsync(&fnode, sizeof(int) * N, c->stream));
     NB2_CUDA(c, cudaMemcpyAsync(c->corder, order.data(), sizeof(int) * E, cudaMemcpyHostToDevice,
                                 c->stream));
-    NB2_CUDA(c, cudaMemcpyAsync(dcol, col.data(), E, cudaMemcpyHostToDevice, c->stream));
-    NB2_CUDA(c, cudaMemsetAsync(fblock, 0x7f, sizeof(int) * c->nnzb, c->stream));
-    NB2_CUDA(c, cudaMemsetAsync(fnode, 0x7f, sizeof(int) * N, c->stream));
-    const int T = 256;
-    const long long mm = (long long)E * npe * npe;
-    k_first_colour<<<(unsigned)((mm + T - 1) / T), T, 0, c->stream>>>(mm, npe, c->slot, c->conn,
-                                                                       dcol, fblock, fnode);
-    k_first_masks<<<(E + T - 1) / T, T, 0, c->stream>>>(E, npe, c->slot, c->conn, dcol, fblock,
-                                                        fnode, c->kfirst, c->ffirst);
-    c->launches += 2;
-    NB2_CUDA(c, cudaGetLastError());
-    // f_int entries of nodes no element references are never written by a coloured pass
-    NB2_CUDA(c, cudaMemsetAsync(c->fint, 0, sizeof(double) * c->n, c->stream));
-    NB2_CUDA(c, cudaFreeAsync(dcol, c->stream));
-    NB2_CUDA(c, cudaFreeAsync(fblock, c->stream));
-    NB2_CUDA(c, cudaFreeAsync(fnode, c->stream));
     NB2_CUDA(c, cudaStreamSynchronize(c->stream));
     c->h_coff = coff;
     c->colour_state = 1;
-    return NB2_OK;
-}
-
-// Element ranges for the red-based FP64 pass (zparts equal ranges in element order).  The K rows
-// a range touches first (its nodes' lowest adjacent element lies in it) are zeroed just before
-// that range runs, so zeroing overlaps the previous range.  Set up only when those rows form one
-// contiguous block range per element range (node order follows element order, as in a
-// structured mesh numbered in the same sweep) and the mesh is large enough to keep each range's
-// launch full.
-int ensure_zero_parts(nb2_ctx* c) {
-    if (c->zstate != 0) return NB2_OK;
-    constexpr int P = 4;
-    c->zstate = -1;
-    if (c->E < 148 * 64 * P) return NB2_OK;
-    NB2_TRY(build_node_adjacency(c));
-    std::vector<int> ptr(c->N + 1), adj((size_t)c->E * c->npe);
-    NB2_CUDA(c, cudaMemcpyAsync(ptr.data(), c->nadj_ptr, sizeof(int) * (c->N + 1),
-                                cudaMemcpyDeviceToHost, c->stream));
-    NB2_CUDA(c, cudaMemcpyAsync(adj.data(), c->nadj, sizeof(int) * adj.size(),
-                                cudaMemcpyDeviceToHost, c->stream));
-    NB2_CUDA(c, cudaStreamSynchronize(c->stream));
-    std::vector<int> pe(P + 1);
-    for (int p = 0; p <= P; ++p) pe[p] = (int)((long long)c->E * p / P);
-    // first range of each node (its slots are sorted, so the first is its lowest element)
-    std::vector<long long> pb(P + 1, -1);
-    int prev = 0;
-    for (int n = 0; n < c->N; ++n) {
-        int fp = prev;
-        if (ptr[n + 1] > ptr[n]) {
-            const int e = adj[ptr[n]] / c->npe;
-            fp = (int)(std::upper_bound(pe.begin(), pe.end(), e) - pe.begin()) - 1;
-        }
-        if (fp < prev) return NB2_OK;  // not monotone: one memset, one launch
-        for (int p = prev + 1; p <= fp; ++p) pb[p] = c->h_brp[n];
-        prev = fp;
-    }
-    pb[0] = 0;
-    for (int p = prev + 1; p <= P; ++p) pb[p] = c->nnzb;
-    for (int p = 1; p <= P; ++p)
-        if (pb[p] < 0) pb[p] = pb[p - 1];
-    NB2_CUDA(c, cudaStreamCreateWithFlags(&c->zstream, cudaStreamNonBlocking));
-    for (int p = 0; p <= P; ++p)
-        NB2_CUDA(c, cudaEventCreateWithFlags(&c->zev[p], cudaEventDisableTiming));
-    c->zpart_e = pe;
-    c->zpart_b = pb;
-    c->zstate = 1;
     return NB2_OK;
 }
 

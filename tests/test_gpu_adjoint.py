@@ -136,8 +136,9 @@ def test_c4_full_size_adjoint(setup):
     sm = api.StaticMatrix(pr)
     u = sm.solve()
     _, g = _objective(pr, u, u_target)
-    grad = sm.mesh.adjoint_shear_gradient(g, api.FP64, 1e-13)
-    g32 = sm.mesh.adjoint_shear_gradient(g, api.MIXED, 1e-13)
+    # the transpose solve at rtol 1e-11 (1e-13 is below what the FP64 PCG reaches at this size)
+    grad = sm.mesh.adjoint_shear_gradient(g, api.FP64, 1e-11)
+    g32 = sm.mesh.adjoint_shear_gradient(g, api.MIXED, 1e-11)
     assert rel_err(g32, grad) < 1e-8
     rng = np.random.Generator(np.random.PCG64(11))
     G0 = pr.element_shear_modulus.copy()
