@@ -214,6 +214,12 @@ int nb2_apply_tangent(nb2_ctx* ctx, const double* v, double* y);
  * FP64 in and out).  Equals nb2_apply_tangent to FP32 rounding.  No reference counterpart. */
 int nb2_apply_tangent_fp32(nb2_ctx* ctx, const double* v, double* y);
 
+/* submesh::tangent_stiffness(element) (submesh.cpp:66-80): one element's tangent stiffness at
+ * the state of the last nb2_update_internal_variables, dense, row-major, in neon's local DOF
+ * order (3a + k for local node a): Ke [3 npe][3 npe] (576 doubles for hex8, 144 for tet4; host).
+ * A per-element getter for checks and debugging; nb2_assemble is the batched path. */
+int nb2_element_stiffness(nb2_ctx* ctx, int64_t element, double* Ke);
+
 /* submesh::save_internal_variables (submesh.cpp:54-64): commit (1) or revert (0). */
 int nb2_save_internal_variables(nb2_ctx* ctx, int32_t converged);
 

@@ -95,6 +95,7 @@ _SIGS = {
     "nb2_last_error": (C.c_int, [P, C.c_char_p, C.c_size_t]),
     "nb2_set_stream": (C.c_int, [P, P]),
     "nb2_set_scatter_mode": (C.c_int, [P, C.c_int32]),
+    "nb2_element_stiffness": (C.c_int, [P, C.c_int64, P]),
     "nb2_get_sizes": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                                 C.POINTER(C.c_int64)]),
     "nb2_launch_count": (C.c_int, [P, C.POINTER(C.c_int64)]),
@@ -322,6 +323,15 @@ class SolidMesh:
                                       int(maximum_iterations), C.byref(it), C.byref(err)),
                self.h, "solve_device")
         return it.value, err.value
+
+    def element_stiffness(self, e: int):
+        """submesh::tangent_stiffness(e): element e's dense tangent [3 npe][3 npe] at the state
+        of the last update_internal_variables (neon's local DOF order 3a + k)."""
+        nd = 3 * self.conn.shape[1]
+        out = np.zeros((nd, nd))
+        _check(lib().nb2_element_stiffness(self.h, int(e), out.ctypes.data), self.h,
+               "element_stiffness")
+        return out
 
     def set_scatter_mode(self, mode: int):
         """SCATTER_RED (fast, run-to-run last-bit differences) or SCATTER_COLOURED (one launch

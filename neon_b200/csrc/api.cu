@@ -141,6 +141,23 @@ int nb2::ensure_k64(nb2_ctx* c) {
     return dev_alloc(c, &c->K64, 9 * c->nnzb);
 }
 
+// The second FP64 K buffer for the double-buffered zeroing; when it does not fit, passes zero
+// their K on the main stream instead (kalt_state -1)
+int nb2::ensure_k64_alt(nb2_ctx* c) {
+    if (c->kalt_state != 0) return NB2_OK;
+    c->kalt_state = -1;
+    if (cudaMalloc(&c->K64_alt, sizeof(double) * 9 * c->nnzb) != cudaSuccess) {
+        cudaGetLastError();  // an allocation failure is not sticky: clear it and go without
+        c->K64_alt = nullptr;
+        return NB2_OK;
+    }
+    NB2_CUDA(c, cudaStreamCreateWithFlags(&c->zstream, cudaStreamNonBlocking));
+    NB2_CUDA(c, cudaEventCreateWithFlags(&c->zev_free, cudaEventDisableTiming));
+    NB2_CUDA(c, cudaEventCreateWithFlags(&c->zev_done, cudaEventDisableTiming));
+    c->kalt_state = 1;
+    return NB2_OK;
+}
+
 extern "C" {
 
 int nb2_create(const nb2_mesh_desc* m, const nb2_material* mat, nb2_ctx** out) {
@@ -228,9 +245,12 @@ int nb2_destroy(nb2_ctx* c) {
                     c->ep_old, c->epbar_old, c->sig, c->dpar,   c->detF,      c->cg_x,
                     c->cg_r,   c->cg_p,   c->cg_q,   c->cg_inv, c->cg32_x,    c->cg32_r,
                     c->cg32_p, c->cg32_q, c->cg32_inv, c->partials, c->cgs,   c->norms,
-                    c->status, c->corder};
+                    c->status, c->corder, c->K64_alt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (c->zev_free) cudaEventDestroy(c->zev_free);
+    if (c->zev_done) cudaEventDestroy(c->zev_done);
+    if (c->zstream) cudaStreamDestroy(c->zstream);
     if (c->h_cgs) cudaFreeHost(c->h_cgs);
     if (c->h_norms) cudaFreeHost(c->h_norms);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -253,6 +273,21 @@ int nb2_set_stream(nb2_ctx* c, void* stream) {
     c->stream = (cudaStream_t)stream;
     c->own_stream = false;
     return NB2_OK;
+}
+
+int nb2_element_stiffness(nb2_ctx* c, int64_t element, double* Ke) {
+    if (!c || !Ke || element < 0 || element >= c->E) return NB2_E_INPUT;
+    const size_t nd = 3 * (size_t)c->npe;
+    double* d = nullptr;
+    NB2_CUDA(c, cudaMallocAsync(&d, sizeof(double) * nd * nd, c->stream));
+    int st = launch_element_stiffness(c, element, d);
+    if (st == NB2_OK) {
+        NB2_CUDA(c, cudaMemcpyAsync(Ke, d, sizeof(double) * nd * nd, cudaMemcpyDeviceToHost,
+                                    c->stream));
+    }
+    cudaFreeAsync(d, c->stream);
+    NB2_CUDA(c, cudaStreamSynchronize(c->stream));
+    return st;
 }
 
 int nb2_set_scatter_mode(nb2_ctx* c, int32_t mode) {

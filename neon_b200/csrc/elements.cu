@@ -35,6 +35,7 @@
 //   phase 3  each lane adds its blocks (and the mirrored lower blocks) with red.global.add into
 //            K[slot], and the force of one node into f_int.
 #include <cmath>
+#include <utility>
 
 #include "nb2_internal.cuh"
 
@@ -545,14 +546,82 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
 //   y_a = s [lam' tr(G) La + mu' (G + G^T) La + b (N:G) N La + (Da eps(G)) La + G sigma La]
 // -- the same tangent the assembled K holds, applied without forming it.
 // ---------------------------------------------------------------------------------------
+// The stored tangent applied at one quadrature point: for the gradient Gm = sum_a v_a (x) L_a of
+// an input v, out[3a + i] = s t_a[i] with
+//   t_a = lam' tr(G) La + mu' (G + G^T) La + b (N:G) N La + (Da eps(G)) La + G sigma La,
+// the point's share of (K_e v)_a (the block formula of the assembled tangent, applied)
+template <int NPE, int MODEL>
+__device__ __forceinline__ void tangent_point_product(const ElementArgs& A, long long q, double s,
+                                                      const double (&L)[NPE][3], const double* Gm,
+                                                      double* out) {
+    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || model_aniso(MODEL));
+    constexpr bool kJ2 = (MODEL == MODEL_J2);
+    constexpr bool kAniso = model_aniso(MODEL);
+    const long long n = A.nqp;
+    const double lam = A.dpar[0 * n + q], mu = A.dpar[1 * n + q];
+    const double trG = Gm[0] + Gm[4] + Gm[8];
+    double bN = 0.0, N6[6] = {0, 0, 0, 0, 0, 0};
+    if constexpr (kJ2) {
+        const double b = A.dpar[2 * n + q];
+        if (b != 0.0) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) N6[c] = A.dpar[(3 + c) * n + q];
+            // N:G with N symmetric (11 22 33 23 13 12)
+            bN = b * (N6[0] * Gm[0] + N6[1] * Gm[4] + N6[2] * Gm[8] +
+                      N6[3] * (Gm[5] + Gm[7]) + N6[4] * (Gm[2] + Gm[6]) +
+                      N6[5] * (Gm[1] + Gm[3]));
+        }
+    }
+    double sa[6] = {0, 0, 0, 0, 0, 0};
+    if constexpr (kAniso) {
+        double Da[21];
+#pragma unroll
+        for (int c = 0; c < 21; ++c) Da[c] = A.dpar[(3 + c) * n + q];
+        aniso_stress(Da, Gm, sa);
+    }
+    double sg[6] = {0, 0, 0, 0, 0, 0};
+    if constexpr (kFinite) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) sg[c] = A.sig[c * n + q];
+    }
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+        const double* La = L[a];
+        double t[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            t[i] = lam * trG * La[i] +
+                   mu * ((Gm[i * 3 + 0] + Gm[0 * 3 + i]) * La[0] +
+                         (Gm[i * 3 + 1] + Gm[1 * 3 + i]) * La[1] +
+                         (Gm[i * 3 + 2] + Gm[2 * 3 + i]) * La[2]);
+        if constexpr (kJ2) {
+            t[0] += bN * (N6[0] * La[0] + N6[5] * La[1] + N6[4] * La[2]);
+            t[1] += bN * (N6[5] * La[0] + N6[1] * La[1] + N6[3] * La[2]);
+            t[2] += bN * (N6[4] * La[0] + N6[3] * La[1] + N6[2] * La[2]);
+        }
+        if constexpr (kAniso) {
+            t[0] += sa[0] * La[0] + sa[5] * La[1] + sa[4] * La[2];
+            t[1] += sa[5] * La[0] + sa[1] * La[1] + sa[3] * La[2];
+            t[2] += sa[4] * La[0] + sa[3] * La[1] + sa[2] * La[2];
+        }
+        if constexpr (kFinite) {
+            const double sl0 = sg[0] * La[0] + sg[5] * La[1] + sg[4] * La[2];
+            const double sl1 = sg[5] * La[0] + sg[1] * La[1] + sg[3] * La[2];
+            const double sl2 = sg[4] * La[0] + sg[3] * La[1] + sg[2] * La[2];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                t[i] += Gm[i * 3 + 0] * sl0 + Gm[i * 3 + 1] * sl1 + Gm[i * 3 + 2] * sl2;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[3 * a + i] = s * t[i];
+    }
+}
+
 template <int NPE, int MODEL>
 __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __restrict__ v,
                                               double* __restrict__ y) {
     using T = Topo<NPE>;
     constexpr int NQ = T::NQ, G = T::G, EPC = T::EPC;
-    constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || model_aniso(MODEL));
-    constexpr bool kJ2 = (MODEL == MODEL_J2);
-    constexpr bool kAniso = model_aniso(MODEL);
     __shared__ double sx[EPC][NPE][3];
     __shared__ double sv[EPC][NPE][3];
     __shared__ double sdN[NQ][NPE][3];
@@ -584,7 +653,6 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
         if (!valid) break;
         const double w = (NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0);
         const long long q = e * NQ + l;
-        const long long n = A.nqp;
         double Fc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int a = 0; a < NPE; ++a)
@@ -608,63 +676,7 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
 #pragma unroll
                 for (int k = 0; k < 3; ++k) Gm[i * 3 + k] += sv[le][a][i] * L[a][k];
         }
-        const double lam = A.dpar[0 * n + q], mu = A.dpar[1 * n + q];
-        const double trG = Gm[0] + Gm[4] + Gm[8];
-        double bN = 0.0, N6[6] = {0, 0, 0, 0, 0, 0};
-        if constexpr (kJ2) {
-            const double b = A.dpar[2 * n + q];
-            if (b != 0.0) {
-#pragma unroll
-                for (int c = 0; c < 6; ++c) N6[c] = A.dpar[(3 + c) * n + q];
-                // N:G with N symmetric (11 22 33 23 13 12)
-                bN = b * (N6[0] * Gm[0] + N6[1] * Gm[4] + N6[2] * Gm[8] +
-                          N6[3] * (Gm[5] + Gm[7]) + N6[4] * (Gm[2] + Gm[6]) +
-                          N6[5] * (Gm[1] + Gm[3]));
-            }
-        }
-        double sa[6] = {0, 0, 0, 0, 0, 0};
-        if constexpr (kAniso) {
-            double Da[21];
-#pragma unroll
-            for (int c = 0; c < 21; ++c) Da[c] = A.dpar[(3 + c) * n + q];
-            aniso_stress(Da, Gm, sa);
-        }
-        double sg[6] = {0, 0, 0, 0, 0, 0};
-        if constexpr (kFinite) {
-#pragma unroll
-            for (int c = 0; c < 6; ++c) sg[c] = A.sig[c * n + q];
-        }
-#pragma unroll
-        for (int a = 0; a < NPE; ++a) {
-            const double* La = L[a];
-            double t[3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-                t[i] = lam * trG * La[i] +
-                       mu * ((Gm[i * 3 + 0] + Gm[0 * 3 + i]) * La[0] +
-                             (Gm[i * 3 + 1] + Gm[1 * 3 + i]) * La[1] +
-                             (Gm[i * 3 + 2] + Gm[2 * 3 + i]) * La[2]);
-            if constexpr (kJ2) {
-                t[0] += bN * (N6[0] * La[0] + N6[5] * La[1] + N6[4] * La[2]);
-                t[1] += bN * (N6[5] * La[0] + N6[1] * La[1] + N6[3] * La[2]);
-                t[2] += bN * (N6[4] * La[0] + N6[3] * La[1] + N6[2] * La[2]);
-            }
-            if constexpr (kAniso) {
-                t[0] += sa[0] * La[0] + sa[5] * La[1] + sa[4] * La[2];
-                t[1] += sa[5] * La[0] + sa[1] * La[1] + sa[3] * La[2];
-                t[2] += sa[4] * La[0] + sa[3] * La[1] + sa[2] * La[2];
-            }
-            if constexpr (kFinite) {
-                const double sl0 = sg[0] * La[0] + sg[5] * La[1] + sg[4] * La[2];
-                const double sl1 = sg[5] * La[0] + sg[1] * La[1] + sg[3] * La[2];
-                const double sl2 = sg[4] * La[0] + sg[3] * La[1] + sg[2] * La[2];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    t[i] += Gm[i * 3 + 0] * sl0 + Gm[i * 3 + 1] * sl1 + Gm[i * 3 + 2] * sl2;
-            }
-#pragma unroll
-            for (int i = 0; i < 3; ++i) sY[le][l][3 * a + i] = s * t[i];
-        }
+        tangent_point_product<NPE, MODEL>(A, q, s, L, Gm, &sY[le][l][0]);
     }
     __syncthreads();
     if (!valid) return;
@@ -684,6 +696,58 @@ __global__ void __launch_bounds__(64) k_apply(ElementArgs A, const double* __res
             atomicAdd(&y[3ll * node[j] + 2], f2);
         }
     }
+}
+
+// One element's tangent stiffness from the stored tangent of the last update, dense
+// [3 NPE][3 NPE] row-major in neon's local DOF order (3a + k): thread j forms column j, the
+// element product with the unit vector e_j, point by point (submesh::tangent_stiffness,
+// submesh.cpp:66-80; a debug getter, one block)
+template <int NPE, int MODEL>
+__global__ void k_element_stiffness(ElementArgs A, long long e, double* __restrict__ Ke) {
+    constexpr int NQ = Topo<NPE>::NQ, ND = 3 * NPE;
+    const int j = threadIdx.x;
+    if (j >= ND) return;
+    double xa[NPE][3];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+        const long long nd = A.conn[e * NPE + a];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) xa[a][k] = A.u[3 * nd + k] + A.X[3 * nd + k];
+    }
+    double col[ND];
+#pragma unroll
+    for (int r = 0; r < ND; ++r) col[r] = 0.0;
+    for (int l = 0; l < NQ; ++l) {
+        const double* dN = (NPE == 8) ? &c_dN_hex8[l * 24] : c_dN_tet4;
+        double Fc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) Fc[i * 3 + k] += xa[a][i] * dN[a * 3 + k];
+        double Ji[9];
+        inv3(Fc, Ji);
+        const double s = ((NPE == 8) ? c_w_hex8[l] : (1.0 / 6.0)) * det3(Fc);
+        double L[NPE][3];
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                L[a][k] = dN[a * 3 + 0] * Ji[0 * 3 + k] + dN[a * 3 + 1] * Ji[1 * 3 + k] +
+                          dN[a * 3 + 2] * Ji[2 * 3 + k];
+        // v = e_j: G = e_i (x) L_b with b = j / 3, i = j % 3
+        double Gm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const int b = j / 3, i = j % 3;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) Gm[i * 3 + k] = L[b][k];
+        double out[ND];
+        tangent_point_product<NPE, MODEL>(A, e * NQ + l, s, L, Gm, out);
+#pragma unroll
+        for (int r = 0; r < ND; ++r) col[r] += out[r];
+    }
+#pragma unroll
+    for (int r = 0; r < ND; ++r) Ke[r * ND + j] = col[r];
 }
 
 #include "mf_kernels.cuh"
@@ -1178,6 +1242,35 @@ int launch_apply(nb2_ctx* c, const double* v, double* y) {
     return NB2_OK;
 }
 
+template <int NPE>
+static void element_stiffness_t(nb2_ctx* c, const ElementArgs& A, long long e, double* Ke) {
+    switch (c->mat.model) {
+        case MODEL_LE: k_element_stiffness<NPE, MODEL_LE><<<1, 32, 0, c->stream>>>(A, e, Ke); break;
+        case MODEL_NH: k_element_stiffness<NPE, MODEL_NH><<<1, 32, 0, c->stream>>>(A, e, Ke); break;
+        case MODEL_J2: k_element_stiffness<NPE, MODEL_J2><<<1, 32, 0, c->stream>>>(A, e, Ke); break;
+        case MODEL_ML: k_element_stiffness<NPE, MODEL_ML><<<1, 32, 0, c->stream>>>(A, e, Ke); break;
+        case MODEL_MN: k_element_stiffness<NPE, MODEL_MN><<<1, 32, 0, c->stream>>>(A, e, Ke); break;
+        default: k_element_stiffness<NPE, MODEL_MS><<<1, 32, 0, c->stream>>>(A, e, Ke); break;
+    }
+    c->launches++;
+}
+
+// Ke_dev [3 npe][3 npe] = element e's tangent stiffness from the tangent stored by the last
+// MODE_STORE pass
+int launch_element_stiffness(nb2_ctx* c, long long e, double* Ke_dev) {
+    int st = upload_tables(c);
+    if (st) return st;
+    if (!c->dpar || !c->u_tan || e < 0 || e >= c->E) return NB2_E_INPUT;
+    ElementArgs A = make_args(c);
+    A.u = c->u_tan;
+    if (c->npe == 8)
+        element_stiffness_t<8>(c, A, e, Ke_dev);
+    else
+        element_stiffness_t<4>(c, A, e, Ke_dev);
+    NB2_CUDA(c, cudaGetLastError());
+    return NB2_OK;
+}
+
 template <int NPE, int MODEL>
 static void mf_setup_t(nb2_ctx* c, const ElementArgs& A) {
     constexpr int EPC = Topo<NPE>::EPC, G = Topo<NPE>::G;
@@ -1345,13 +1438,29 @@ int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
         NB2_TRY(ensure_colouring(c));
         coloured = c->colour_state == 1;
     }
-    ElementArgs A = make_args(c);
+    // FP64 K of one problem is double-buffered: the buffer zeroed in the background during the
+    // previous pass becomes K, and the previous K is zeroed during this pass (it is no longer
+    // read once the work queued before this pass is done)
+    const bool kdouble = (mode & MODE_STIFFNESS) && precision == NB2_FP64 && !c->e_inst;
+    if (kdouble) NB2_TRY(ensure_k64_alt(c));
+    const bool kbg = kdouble && c->kalt_state == 1;
     if (mode & MODE_STIFFNESS) {
-        if (precision == NB2_FP64)
+        if (kbg && c->alt_zeroed) {
+            std::swap(c->K64, c->K64_alt);
+            c->kbuf ^= 1;
+            NB2_CUDA(c, cudaStreamWaitEvent(c->stream, c->zev_done, 0));
+            c->alt_zeroed = false;
+        } else if (precision == NB2_FP64) {
             NB2_CUDA(c, cudaMemsetAsync(c->K64, 0, sizeof(double) * 9 * c->nnzb, c->stream));
-        else
+        } else {
             NB2_CUDA(c, cudaMemsetAsync(c->K32, 0, sizeof(float) * 9 * c->nnzb, c->stream));
+        }
     }
+    if (kbg) {
+        NB2_CUDA(c, cudaEventRecord(c->zev_free, c->stream));
+        NB2_CUDA(c, cudaStreamWaitEvent(c->zstream, c->zev_free, 0));
+    }
+    ElementArgs A = make_args(c);
     if (mode & MODE_FORCE) NB2_CUDA(c, cudaMemsetAsync(c->fint, 0, sizeof(double) * c->n, c->stream));
     if (coloured) {
         // one launch per colour: an entry of K or f_int receives at most one term per launch,
@@ -1366,6 +1475,11 @@ int launch_element_kernel(nb2_ctx* c, int mode, int precision) {
         st = (c->npe == 8) ? dispatch_model<8>(c, A, mode, precision)
                            : dispatch_model<4>(c, A, mode, precision);
         if (st) return st;
+    }
+    if (kbg) {
+        NB2_CUDA(c, cudaMemsetAsync(c->K64_alt, 0, sizeof(double) * 9 * c->nnzb, c->zstream));
+        NB2_CUDA(c, cudaEventRecord(c->zev_done, c->zstream));
+        c->alt_zeroed = true;
     }
     // the matrix-free tangent re-derives the gradients from this displacement, not from a
     // later one (the Newton step adds the prescribed increment before its first solve)

@@ -175,7 +175,16 @@ struct nb2_ctx {
     double* h_norms = nullptr;        // pinned mirror
     nb2::DeviceStatus* status = nullptr;
 
-    cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;  // captured CG iteration blocks
+    // captured CG iteration blocks; the FP64 one per K buffer (the graph holds the K pointer)
+    cudaGraphExec_t graph64[2] = {nullptr, nullptr}, graph32 = nullptr;
+    // double-buffered K zeroing (FP64 stiffness passes of one problem): while a pass assembles
+    // into K64, the previous K (K64_alt) is zeroed on zstream for the next pass
+    double* K64_alt = nullptr;
+    int kbuf = 0;            // which of the two buffers K64 is (selects graph64)
+    bool alt_zeroed = false; // K64_alt's zeroing is queued (zev_done marks its end)
+    int kalt_state = 0;      // 0 not set up, 1 ready, -1 off (the second buffer did not fit)
+    cudaStream_t zstream = nullptr;
+    cudaEvent_t zev_free = nullptr, zev_done = nullptr;
 
     // batched solves: set for the duration of one (device arrays owned by the batch state)
     const int* e_inst = nullptr;
@@ -209,6 +218,7 @@ int cuda_fail(nb2_ctx* c, cudaError_t e, const char* what);
 
 // api.cu: lazily allocated buffers and the element status word
 int ensure_k64(nb2_ctx* c);            // K64
+int ensure_k64_alt(nb2_ctx* c);        // the second K buffer, its stream and events
 int ensure_k32(nb2_ctx* c);            // K32 and the FP32 CG vectors
 int ensure_cg32(nb2_ctx* c);           // the FP32 CG vectors only (matrix-free mixed PCG)
 int ensure_split_buffers(nb2_ctx* c);  // stored quadrature-point outputs + their displacement
@@ -224,6 +234,7 @@ int export_csr_values(nb2_ctx* c, const double* Kbsr, double* Kcsr_dev);
 // elements.cu
 int launch_element_kernel(nb2_ctx* c, int mode, int precision);
 int launch_apply(nb2_ctx* c, const double* v, double* y);  // y = K v, FP64 matrix-free
+int launch_element_stiffness(nb2_ctx* c, long long e, double* Ke_dev);  // one dense K_e
 int launch_adjoint_shear(nb2_ctx* c, const double* lam, double* dJdG);
 int launch_force_jvp(nb2_ctx* c, const double* v, double* y);  // exact (d f_int/du) v
 int launch_mf_setup(nb2_ctx* c);  // FP32 matrix-free data + diagonal contributions

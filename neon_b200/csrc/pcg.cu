@@ -845,7 +845,7 @@ int pcg_device_fp64(nb2_ctx* c, const double* b, double* x, double tol, int maxi
                     int* iterations, double* error, bool use_graphs) {
     return run_bsr_cg<double, double>(c, c->K64, c->cg_x, c->cg_r, c->cg_p, c->cg_q, c->cg_inv, b,
                                       x, tol, maxit, use_mask, iterations, error,
-                                      use_graphs && use_mask, &c->graph64);
+                                      use_graphs && use_mask, &c->graph64[c->kbuf]);
 }
 
 int pcg_device_fp32(nb2_ctx* c, const double* b, double* x, double tol, int maxit, int* iterations,
@@ -856,10 +856,13 @@ int pcg_device_fp32(nb2_ctx* c, const double* b, double* x, double tol, int maxi
 }
 
 void release_graphs(nb2_ctx* c) {
-    if (c->graph64) cudaGraphExecDestroy(c->graph64);
+    for (auto& g : c->graph64) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
     if (c->graph32) cudaGraphExecDestroy(c->graph32);
     if (c->graph_mf) cudaGraphExecDestroy(c->graph_mf);
-    c->graph64 = c->graph32 = c->graph_mf = nullptr;
+    c->graph32 = c->graph_mf = nullptr;
 }
 
 // y = K v with the FP32 matrix-free operator (v, y device FP64; y unmasked)

@@ -303,3 +303,28 @@ def test_cpp_adapter_driver(api, oracle):
     assert rep["status"] == 0
     assert out["newton_iterations"] == rep["newton_iterations"]
     assert rel_err(np.array(out["u"]), u_o) < 1e-10
+
+
+@pytest.mark.parametrize("topo", ["hex8", "tet4"])
+@pytest.mark.parametrize("model", ["linear_elastic", "neohooke", "j2", "microsphere", "langevin",
+                                   "nonaffine"])
+def test_element_stiffness_getter(api, oracle, topo, model):
+    """nb2_element_stiffness (submesh::tangent_stiffness(e)) equals the oracle's element matrix
+    in neon's local DOF order; an element index past the end is refused."""
+    m = _meshes()[topo]
+    mat = MATERIALS[model]
+    Ge = None
+    if model in FIELD_MODELS:
+        Ge = np.random.Generator(np.random.PCG64(5)).lognormal(0.0, 0.3, m.num_elements)
+    g = api.SolidMesh(m.X, m.conn, mat, Ge)
+    om = oracle.OracleMesh(m.X, m.conn, mat, Ge)
+    u = random_displacement(m, SCALE[model], 21)
+    assert om.update(u)[0] == 0
+    g.update_internal_variables(u)
+    for e in (0, m.num_elements // 2, m.num_elements - 1):
+        Ke = g.element_stiffness(e)
+        Ko = om.element_stiffness(e)
+        assert Ke.shape == Ko.shape == (3 * m.nodes_per_element,) * 2
+        assert rel_err(Ke, Ko) < TOL_K
+    with pytest.raises(ValueError):
+        g.element_stiffness(m.num_elements)
