@@ -241,7 +241,7 @@ int nb2_destroy(nb2_ctx* c) {
     void* ptrs[] = {c->X,      c->conn,   c->brp,    c->bcol,   c->slot,      c->K64,
                     c->K32,    c->u,      c->u_old,  c->fint,   c->fext,      c->rhs,
                     c->du,     c->inc,    c->mask,   c->Ge,     c->Ke,        c->ep,
-                    c->epbar,  c->u_tan, c->Kcsr, c->mf_d, c->mf_c, c->mf_ye, c->nadj, c->nadj_ptr,
+                    c->epbar,  c->u_tan, c->Kcsr, c->mf_d, c->mf_c, c->mf_ye, c->nadj, c->nadj_ptr, c->nadj_pl,
                     c->ep_old, c->epbar_old, c->sig, c->dpar,   c->detF,      c->cg_x,
                     c->cg_r,   c->cg_p,   c->cg_q,   c->cg_inv, c->cg32_x,    c->cg32_r,
                     c->cg32_p, c->cg32_q, c->cg32_inv, c->partials, c->cgs,   c->norms,

@@ -9,7 +9,8 @@
 // input/output vectors.
 //   k_mf_setup  once per linear solve (after an element pass that stored its outputs): writes
 //               those FP32 data and each element's contribution to diag(K) (Jacobi);
-//   k_apply32   per CG iteration: y_e = K_e v_e in FP32, written per element (ye[E][npe*3]);
+//   k_apply32   per CG iteration: y_e = K_e v_e in FP32, written per local node plane
+//               (ye[npe][E][3]);
 //               a node-ordered gather (pcg.cu) sums ye into q without atomics, in a fixed order.
 // With G = sum_b v_b (x) L_b the element force of node a is (the product the assembled blocks
 //   K_ab = s[lam' La(x)Lb + mu'((La.Lb) I + Lb(x)La) + b (N La)(x)(N Lb)] + s (La.sigma.Lb) I
@@ -48,7 +49,7 @@ struct MfCoef {
 //   md[e][3a+k]  = (float)(x_a - x_0)_k
 //   mc[c][q]     = s lam', s mu' | J2: s b, N (6) | finite strain: s sigma (6)
 //                  | Langevin / non-affine microsphere: then s Da (21, packed upper triangle)
-//   de[e][3a+i]  = element contribution to K_(3a+i, 3a+i)
+//   de[a][e][i]  = element contribution to K_(3a+i, 3a+i) (the per-node planes of ye)
 template <int NPE, int MODEL>
 __global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restrict__ md,
                                                  float* __restrict__ mc, float* __restrict__ de) {
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restric
                 double t = 0.0;
 #pragma unroll
                 for (int l = 0; l < NQ; ++l) t += sD[le][l][3 * a + i];
-                de[e * NPE * 3 + 3 * a + i] = (float)t;
+                de[((long long)a * A.E + e) * 3 + i] = (float)t;
             }
     }
 }
@@ -411,9 +412,9 @@ k_apply32(int E, const int* __restrict__ conn,
             }
         }
     }
-    float4* o4 = reinterpret_cast<float4*>(ye + e * NPE * 3);
+    // one plane per local node: threads of consecutive elements write consecutive entries
 #pragma unroll
-    for (int j = 0; j < NPE * 3 / 4; ++j)
-        o4[j] = make_float4((&y[0][0])[4 * j + 0], (&y[0][0])[4 * j + 1], (&y[0][0])[4 * j + 2],
-                            (&y[0][0])[4 * j + 3]);
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) ye[((long long)a * E + e) * 3 + i] = y[a][i];
 }

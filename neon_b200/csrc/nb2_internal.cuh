@@ -153,9 +153,10 @@ struct nb2_ctx {
     // coefficients, per-element products / diagonal contributions, node -> element-slot lists
     float* mf_d = nullptr;   // [E][npe*3]
     float* mf_c = nullptr;   // [kc][nqp]
-    float* mf_ye = nullptr;  // [E][npe*3]
+    float* mf_ye = nullptr;  // [npe][E][3]: one plane per local node (coalesced on both sides)
     int* nadj_ptr = nullptr; // [N+1]
     int* nadj = nullptr;     // [E*npe] element slots e*npe + a, grouped by node
+    int* nadj_pl = nullptr;  // [E*npe] the same slots as plane positions a*E + e of mf_ye
     // colour-partitioned launches (hex8, single problem): elements grouped by colour
     int* corder = nullptr;                   // [E] elements sorted by colour
     std::vector<int> h_coff;                 // colour offsets into corder

@@ -515,7 +515,9 @@ __global__ void __launch_bounds__(kRedThreads) k_bsr_apply(Bsr<V> A, const doubl
 // ---------------------------------------------------------------------------------------
 // matrix-free FP32 operator: node-ordered gather of the per-element products
 // ---------------------------------------------------------------------------------------
-// q = sum over the node's element slots of ye (masked rows 0), p.q -> alpha (as k_spmv)
+// q = sum over the node's element slots of ye (masked rows 0), p.q -> alpha (as k_spmv).  nadj
+// holds each slot's position in ye's per-node planes, so neighbouring nodes read neighbouring
+// elements' entries of one plane (coalesced)
 template <typename X>
 __global__ void __launch_bounds__(kRedThreads) k_mf_gather(int N, const int* __restrict__ nptr,
                                                            const int* __restrict__ nadj,
@@ -640,7 +642,7 @@ struct CgRunner {
                 if (mf) {
                     enqueue_apply32(c, p, c->mf_ye, &c->cgs->done);
                     k_mf_gather<X><<<RB, kRedThreads, 0, c->stream>>>(
-                        c->N, c->nadj_ptr, c->nadj, c->mf_ye, p, q, c->mask, c->cgs, c->partials);
+                        c->N, c->nadj_ptr, c->nadj_pl, c->mf_ye, p, q, c->mask, c->cgs, c->partials);
                     k_xr<X><<<RB, kRedThreads, 0, c->stream>>>(n, x, r, p, q, inv, c->cgs,
                                                                c->partials);
                     k_p<X><<<RB, kRedThreads, 0, c->stream>>>(n, p, r, inv, c->cgs);
@@ -769,7 +771,7 @@ int pcg_reliable_mixed(nb2_ctx* c, const double* b, double* x, double tol, doubl
         // FP32 operator data and the Jacobi inverse from the stored tangent
         NB2_TRY(ensure_mf(c));
         NB2_TRY(launch_mf_setup(c));
-        k_mf_diag<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->nadj_ptr, c->nadj,
+        k_mf_diag<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->nadj_ptr, c->nadj_pl,
                                                              c->mf_ye, c->cg32_inv);
         c->launches++;
     }
@@ -874,10 +876,19 @@ int mf_apply(nb2_ctx* c, const double* v, double* y) {
     k_to_float<<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 8), 256, 0, c->stream>>>(
         n, v, c->cg32_p);
     enqueue_apply32(c, c->cg32_p, c->mf_ye, nullptr);
-    k_mf_sum<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->nadj_ptr, c->nadj, c->mf_ye, y);
+    k_mf_sum<<<(c->N + 255) / 256, 256, 0, c->stream>>>(c->N, c->nadj_ptr, c->nadj_pl, c->mf_ye, y);
     c->launches += 3;
     NB2_CUDA(c, cudaGetLastError());
     return NB2_OK;
+}
+
+// slot e*npe + a of the node adjacency -> its position a*E + e in the per-node planes of mf_ye
+__global__ void k_plane_slots(long long m, int npe, int E, const int* __restrict__ nadj,
+                              int* __restrict__ nadj_pl) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const int sl = nadj[k];
+    nadj_pl[k] = (sl % npe) * E + sl / npe;
 }
 
 int ensure_mf(nb2_ctx* c) {
@@ -887,7 +898,14 @@ int ensure_mf(nb2_ctx* c) {
     NB2_CUDA(c, cudaMalloc(&c->mf_ye, sizeof(float) * ev));
     NB2_CUDA(c, cudaMalloc(&c->mf_c, sizeof(float) * (long long)mf_coefficients(c->mat.model) *
                                          c->nqp));
-    return build_node_adjacency(c);
+    NB2_TRY(build_node_adjacency(c));
+    const long long m = (long long)c->E * c->npe;
+    NB2_CUDA(c, cudaMalloc(&c->nadj_pl, sizeof(int) * m));
+    k_plane_slots<<<(unsigned)((m + 255) / 256), 256, 0, c->stream>>>(m, c->npe, c->E, c->nadj,
+                                                                       c->nadj_pl);
+    c->launches++;
+    NB2_CUDA(c, cudaGetLastError());
+    return NB2_OK;
 }
 
 void bsr_spmv_fp64(nb2_ctx* c, const double* x, double* y, bool use_mask) {
