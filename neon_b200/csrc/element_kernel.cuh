@@ -105,6 +105,13 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
         double Ji[9], s = 0.0;
         if (active) {
             const long long q = e * NQ + l;
+            // the J2 history is loaded first, so its loads overlap the geometry below
+            double ep_q[6] = {0, 0, 0, 0, 0, 0}, ebar_q = 0.0;
+            if constexpr (kJ2 && kCon) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) ep_q[c] = A.ep[c * (long long)A.nqp + q];
+                ebar_q = A.epbar[q];
+            }
             // one pass over the nodes: F0 = X dN and U = (x - X) dN, then the current
             // Jacobian F = x dN = F0 + U, H = U F0^-1 (= sum_a (x_a - X_a) (x) (dN_a F0^-1),
             // submesh.cpp:225-231); without the update only F
@@ -163,7 +170,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                 } else if constexpr (MODEL == MODEL_NH) {
                     cm_neo_hooke(Ae, Fd, detF, o);
                 } else if constexpr (MODEL == MODEL_J2) {
-                    if (!cm_j2(A, q, Hm, o)) report_status(A, e, NB2_E_RETURN_MAP);
+                    if (!cm_j2(A, q, Hm, o, ep_q, ebar_q)) report_status(A, e, NB2_E_RETURN_MAP);
                 } else if constexpr (MODEL == MODEL_MS) {
                     cm_microsphere(Ae, Ae.G, Fd, detF, o);
                 } else if constexpr (MODEL == MODEL_ML) {

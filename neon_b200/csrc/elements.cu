@@ -176,15 +176,17 @@ __device__ __forceinline__ void cm_neo_hooke(const ElementArgs& A, const double*
     o.b = 0.0;
 }
 
-// small_strain_J2_plasticity.cpp:30-163; the current plastic state is mutated on every call
+// small_strain_J2_plasticity.cpp:30-163; the current plastic state is mutated on every call.
+// ep_in / ebar_in: the point's plastic strain and accumulated plastic strain, loaded by the
+// caller ahead of its geometry so the loads overlap it
 __device__ __forceinline__ bool cm_j2(const ElementArgs& A, long long q, const double* H,
-                                      QpOut& o) {
+                                      QpOut& o, const double* ep_in, double ebar_in) {
     const double G = A.G, lam = A.lambda, Hh = A.H_iso;
     const long long n = A.nqp;
     double ep[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) ep[c] = A.ep[c * n + q];
-    double ebar = A.epbar[q];
+    for (int c = 0; c < 6; ++c) ep[c] = ep_in[c];
+    double ebar = ebar_in;
     double e0 = H[0] - ep[0], e1 = H[4] - ep[1], e2 = H[8] - ep[2];
     double e3 = 0.5 * (H[5] + H[7]) - ep[3], e4 = 0.5 * (H[2] + H[6]) - ep[4],
            e5 = 0.5 * (H[1] + H[3]) - ep[5];
