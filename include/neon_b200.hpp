@@ -134,6 +134,16 @@ struct dof_table {
     std::vector<double> times, values, weights;
 };
 
+class mesh;  // a part read from neon's deck and .mesh file (neon_b200_json.hpp)
+
+/// How a deck that asks for a direct linear solver ("direct", "PaStiX", "MUMPS") is solved:
+/// refused (the default), or by the PCG at the given settings.
+struct direct_solver_substitute {
+    bool allowed = false;
+    double tolerance = 1.0e-10;
+    std::int32_t maximum_iterations = 20000;
+};
+
 /// Full-Newton quasi-static solver with adaptive load stepping.
 class static_matrix {
 public:
@@ -141,6 +151,14 @@ public:
                   std::vector<dof_table> dirichlet, std::vector<dof_table> nodal_forces = {})
         : mesh(mesh), options(options), dirichlet(std::move(dirichlet)),
           forces(std::move(nodal_forces)) {}
+
+    /// static_matrix(mesh_type&, json const& simulation) (static_matrix.hpp:109-143): the
+    /// options from the step's "nonlinear_options", "time" and "linear_solver"; the boundaries
+    /// from the part.  Defined in neon_b200_json.hpp.
+    template <class Json>
+    static_matrix(::neon_b200::mesh& part, Json const& simulation,
+                  std::int32_t precision = NB2_FP64,
+                  direct_solver_substitute const& direct = direct_solver_substitute{});
 
     void solve() {
         auto pack = [](std::vector<dof_table> const& in) {

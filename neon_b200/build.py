@@ -71,13 +71,34 @@ def build_adapter_driver(force: bool = False) -> str:
     library with an $ORIGIN rpath so it runs from the tree."""
     lib = build()
     src = os.path.join(ROOT, "tests", "cpp", "adapter_driver.cpp")
-    deps = [src, lib, os.path.join(ROOT, "include", "neon_b200.hpp")]
+    deps = [src, lib, os.path.join(ROOT, "include", "neon_b200.hpp"),
+            os.path.join(ROOT, "include", "neon_b200_json.hpp")]
     if force or _stale(DRIVER, deps):
         cmd = [shutil.which("g++") or "g++", "-std=c++17", "-O2", src, "-o", DRIVER,
                "-I" + os.path.join(ROOT, "include"), "-L" + LIBDIR, "-lneon_b200",
                "-Wl,-rpath,$ORIGIN"]
+        inc = nlohmann_include()
+        if inc:
+            cmd += ["-DNB2_DRIVER_JSON", "-I" + inc]
         subprocess.run(cmd, check=True)
     return DRIVER
+
+
+def nlohmann_include() -> str | None:
+    """A directory holding nlohmann/json.hpp (the JSON library neon uses), for the driver's deck
+    mode: $NLOHMANN_JSON_INCLUDE, the system include paths, or a copy that a Python package in
+    this environment vendors.  None when there is none."""
+    cands = [os.environ.get("NLOHMANN_JSON_INCLUDE", ""), "/usr/include", "/usr/local/include"]
+    import site
+    import sysconfig
+    roots = {sysconfig.get_paths()["purelib"], *site.getsitepackages()}
+    for r in sorted(roots):
+        cands += [os.path.join(r, "include", "cudnn_frontend", "thirdparty"),
+                  os.path.join(r, "include")]
+    for c in cands:
+        if c and os.path.isfile(os.path.join(c, "nlohmann", "json.hpp")):
+            return c
+    return None
 
 
 if __name__ == "__main__":

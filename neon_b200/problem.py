@@ -143,14 +143,56 @@ class DofTable:
 
 
 def sinusoidal_table(amplitude, period, number_of_cycles, phase, generate_time_step):
-    """boundary::generate_sinusoidal (mesh/boundary/boundary.cpp:87-147) for one block."""
-    omega = 2.0 * math.pi / period
-    steps = int(number_of_cycles * period / generate_time_step)
-    block = np.arange(1, steps + 1, dtype=np.float64)
-    scale = number_of_cycles * period / block[-1]
-    t = block * scale + 0.0
-    v = amplitude * np.sin(omega * t + phase)
-    return np.concatenate([[0.0], t]), np.concatenate([[0.0], v])
+    """boundary::generate_sinusoidal (mesh/boundary/boundary.cpp:87-147): a time/value table that
+    starts at (0, 0) and appends one block of sampled sine cycles per entry of the four lists
+    (scalars are one block).  Each block has floor(cycles * period / generate_time_step) samples
+    spread evenly over its cycles and starts where the previous block ended."""
+    lists = [np.atleast_1d(np.asarray(a, dtype=np.float64))
+             for a in (amplitude, period, number_of_cycles, phase)]
+    if len({len(a) for a in lists}) != 1:
+        raise ValueError("The amplitude, period, number_of_cycles, time_step and phase vectors "
+                         "must be of the same size.")
+    times, values = [0.0], [0.0]
+    for A, T, n, ph in zip(*lists):
+        omega = 2.0 * math.pi / T
+        steps = int(n * T / generate_time_step)
+        block = np.arange(1, steps + 1, dtype=np.float64)
+        t = block * (n * T / block[-1]) + times[-1]
+        times.extend(t.tolist())
+        values.extend((A * np.sin(omega * t + ph)).tolist())
+    return np.asarray(times), np.asarray(values)
+
+
+def time_value_table(times, values):
+    """boundary::allocate_time_load (mesh/boundary/boundary.cpp:150-176): at least two points,
+    equal lengths, times non-decreasing."""
+    t = np.asarray(times, dtype=np.float64).reshape(-1)
+    v = np.asarray(values, dtype=np.float64).reshape(-1)
+    if t.size < 2:
+        raise ValueError('"time" is not a vector of at least two elements')
+    if v.size < 2:
+        raise ValueError("The specified boundary values do not contain at least two elements")
+    if t.size != v.size:
+        raise ValueError("The time and load vectors must be of the same size.")
+    if np.any(np.diff(t) < 0.0):
+        raise ValueError("Load times must be monotonically increasing.")
+    return t, v
+
+
+def boundary_table(boundary: dict, key: str, generate_time_step: float):
+    """The time/value table of one component of a boundary (boundary.cpp:20-34): neon's
+    sinusoidal generator when ``generate_type`` is "sinusoidal", else ``time`` and the
+    component's values."""
+    if "generate_type" in boundary:
+        if boundary["generate_type"] != "sinusoidal":
+            raise ValueError(f'"generate_type" {boundary["generate_type"]!r} is not supported')
+        for field in ("period", "phase", "number_of_cycles"):
+            if field not in boundary:
+                raise ValueError(f'"{field}" was not specified in "boundaries".')
+        t, v = sinusoidal_table(boundary[key], boundary["period"], boundary["number_of_cycles"],
+                                boundary["phase"], generate_time_step)
+        return time_value_table(t, v)
+    return time_value_table(boundary["time"], boundary[key])
 
 
 def dirichlet_boundaries(mesh: Mesh, boundaries: list, generate_time_step: float = 1.0):
@@ -166,11 +208,7 @@ def dirichlet_boundaries(mesh: Mesh, boundaries: list, generate_time_step: float
         for comp, key in enumerate("xyz"):
             if key not in b:
                 continue
-            if b.get("generate_type") == "sinusoidal":
-                t, v = sinusoidal_table(b[key][0], b["period"][0], b["number_of_cycles"][0],
-                                        b["phase"][0], generate_time_step)
-            else:
-                t, v = np.asarray(b["time"], float), np.asarray(b[key], float)
+            t, v = boundary_table(b, key, generate_time_step)
             out.append(DofTable((3 * nodes + comp).astype(np.int32), t, v, name=b["name"]))
     return out
 
@@ -207,18 +245,14 @@ def nonfollower_loads(mesh: Mesh, boundaries: list, generate_time_step: float = 
         if kind == "pressure":
             if "value" not in b:
                 raise ValueError('Pressure boundary condition must specify a "value" array')
-            out.append(LoadSpec(PRESSURE, np.asarray(b["time"], float),
-                                np.asarray(b["value"], float), 0, mesh.faces[b["name"]],
+            t, v = time_value_table(b["time"], b["value"])
+            out.append(LoadSpec(PRESSURE, t, v, 0, mesh.faces[b["name"]],
                                 reduced, b["name"]))
             continue
         for comp, key in enumerate("xyz"):
             if key not in b:
                 continue
-            if b.get("generate_type") == "sinusoidal":
-                t, v = sinusoidal_table(b[key][0], b["period"][0], b["number_of_cycles"][0],
-                                        b["phase"][0], generate_time_step)
-            else:
-                t, v = np.asarray(b["time"], float), np.asarray(b[key], float)
+            t, v = boundary_table(b, key, generate_time_step)
             if kind == "traction":
                 out.append(LoadSpec(TRACTION, t, v, comp, mesh.faces[b["name"]], reduced,
                                     b["name"]))

@@ -1,0 +1,56 @@
+"""A neon input deck solved end to end through the C++ adapter (include/neon_b200_json.hpp:
+basic_mesh -> mesh -> static_matrix(mesh, simulation).solve(), tests/cpp/adapter_driver.cpp)
+and through the Python reader (neon_b200.deck -> api.StaticMatrix): the same device path, so the
+displacements agree bit for bit, and both agree with the oracle's static_matrix solve."""
+import numpy as np
+import pytest
+
+from conftest import (cube_example_deck, cube_mesh_file, loaded_block_deck, rel_err,
+                      run_adapter_driver)
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "block_hex8_neohooke": lambda: loaded_block_deck("hex8", "neohooke"),
+    "block_tet4_neohooke": lambda: loaded_block_deck("tet4", "neohooke"),
+    "block_hex8_j2": lambda: loaded_block_deck("hex8", "j2"),
+    "block_tet4_j2": lambda: loaded_block_deck("tet4", "j2"),
+    "neohooke_cube_example": lambda: (cube_example_deck("neohooke_cube_example"),
+                                      cube_mesh_file()),
+}
+
+
+@pytest.fixture(scope="module")
+def api():
+    from neon_b200 import api as A
+    A.lib()
+    return A
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_cpp_deck_solve(tmp_path, api, oracle, case):
+    from neon_b200 import deck as D
+    deck, mesh_file = CASES[case]()
+    direct = (1e-10, 20000)
+    out = run_adapter_driver(tmp_path, deck, mesh_file, "--direct", repr(direct[0]),
+                             str(direct[1]))
+    if out is None:
+        pytest.skip("the adapter driver was built without nlohmann/json.hpp")
+    assert "error" not in out, out
+    pr = D.problem_from_deck(deck, mesh_file, direct_solver=direct)
+    sm = api.StaticMatrix(pr)
+    u = sm.solve()
+    # the load tables the C++ mesh built (nodal forces, then non-follower loads with their
+    # device-computed weights) are the ones the Python route builds
+    tables = sm.external_force_tables()
+    assert len(out["forces"]) == len(tables)
+    for c, t in zip(out["forces"], tables):
+        assert np.array_equal(c["dofs"], t.dofs)
+        w = np.ones(len(t.dofs)) if t.weights is None else t.weights
+        assert np.array_equal(np.asarray(c["weights"] or np.ones(len(t.dofs))), w)
+    u_cpp = np.asarray(out["u"])
+    assert sm.report["status"] == 0, sm.report["message"]
+    assert out["newton_iterations"] == sm.report["newton_iterations"]
+    assert np.array_equal(u_cpp, u), rel_err(u_cpp, u)
+    _, u_o, _, _, _ = oracle.static_solve(pr)
+    assert rel_err(u, u_o) < 1e-10
