@@ -434,8 +434,9 @@ def main():
     mesh.set_scatter_mode(api.SCATTER_RED)
     coloured = {"ms_per_step": sum(col_ms) / len(col_ms),
                 "elements_per_s": E / (sum(col_ms) / len(col_ms) * 1e-3),
-                "note": "one launch per element colour, first term stored, later colours added: "
-                        "bit-reproducible K and f_int (nb2_static_solve always uses it)"}
+                "note": "K and f_int zeroed, then one launch per element colour adding into them "
+                        "(no entry gets two additions in one launch, so every sum runs in colour "
+                        "order): bit-reproducible K and f_int (nb2_static_solve always uses it)"}
 
     # roofline of the dominant kernel (the fused element kernel)
     peaks = {}
@@ -620,7 +621,10 @@ def newton_comparison(api, P, args, mesh_unused):
       yielding         the first `newton_load_steps` increments (points yield);
       cyclic           the first `newton_cyclic_increments` increments of the 80-increment
                        cycle (24 = t in [0, 6]: past the load reversal at t = 5, where the top
-                       face starts to unload); 80 runs the whole cycle.
+                       face starts to unload); 80 runs the whole cycle.  Increments that do not
+                       converge are halved (neon's adaptive stepping), so the segment's Newton
+                       iterations include those of the failed attempts; `completed` says both
+                       paths reached the segment's end time.
     The reference's J2 update mutates the plastic strain at every Newton iteration, so once
     points yield the converged displacement depends on the Newton path.  The FP64 path is bit
     reproducible (fixed-order assembly and reductions): `fp64_rerun_rel_err_u` is that check;
@@ -640,6 +644,7 @@ def newton_comparison(api, P, args, mesh_unused):
         u32, r32 = _newton_run(api, P, args.size, steps, api.MIXED, delta)
         log(f"newton {name} mixed: {r32['seconds_total']:.2f} s")
         seg = {"load_steps_run": steps, "fp64": r64, "mixed": r32,
+               "completed": r64["status"] == 0 and r32["status"] == 0,
                "mixed_rel_err_u": _rel(u32, u64),
                "newton_step_speedup": r64["newton_step_s"] / max(r32["newton_step_s"], 1e-12),
                "solve_speedup": r64["seconds_total"] / max(r32["seconds_total"], 1e-12)}
