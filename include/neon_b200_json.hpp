@@ -328,7 +328,7 @@ nb2_solver_options make_solver_options(Json const& simulation, std::int32_t prec
                                 "\"iterative\")");
     }
     o.precision = precision;
-    o.mixed_inner_tolerance = 1.0e-3;
+    o.mixed_inner_tolerance = 1.0e-2;
     o.use_graphs = 1;
     return o;
 }

@@ -418,7 +418,7 @@ def _tables(tables, keep):
 class StaticMatrix:
     """mechanics::static_matrix: full Newton with adaptive load stepping on the device."""
 
-    def __init__(self, problem: Problem, precision=FP64, mixed_inner_tolerance=1e-6,
+    def __init__(self, problem: Problem, precision=FP64, mixed_inner_tolerance=1e-2,
                  use_graphs=True, mesh: SolidMesh | None = None):
         self.problem = problem
         m = problem.mesh
