@@ -1,7 +1,8 @@
 """A neon input deck solved end to end through the C++ adapter (include/neon_b200_json.hpp:
 basic_mesh -> mesh -> static_matrix(mesh, simulation).solve(), tests/cpp/adapter_driver.cpp)
 and through the Python reader (neon_b200.deck -> api.StaticMatrix): the same device path, so the
-displacements agree bit for bit, and both agree with the oracle's static_matrix solve."""
+displacements agree bit for bit on hexahedra (colour-ordered element passes) and to rounding on
+tetrahedra, and both agree with the oracle's static_matrix solve."""
 import numpy as np
 import pytest
 
@@ -51,6 +52,12 @@ def test_cpp_deck_solve(tmp_path, api, oracle, case):
     u_cpp = np.asarray(out["u"])
     assert sm.report["status"] == 0, sm.report["message"]
     assert out["newton_iterations"] == sm.report["newton_iterations"]
-    assert np.array_equal(u_cpp, u), rel_err(u_cpp, u)
+    if pr.mesh.nodes_per_element == 8:
+        # hex8 element passes run in colour order inside the Newton driver: the same bits
+        assert np.array_equal(u_cpp, u), rel_err(u_cpp, u)
+    else:
+        # tet4 passes add with atomics in arrival order; through neon's path-dependent J2
+        # update the last bits move the converged displacement at the 1e-13 level
+        assert rel_err(u_cpp, u) < 1e-10
     _, u_o, _, _, _ = oracle.static_solve(pr)
     assert rel_err(u, u_o) < 1e-10
