@@ -1316,8 +1316,8 @@ int mf_coefficients(int model) {
 template <int NPE, int MODEL>
 static void apply32_t(nb2_ctx* c, const float* v, float* ye, const int* done) {
     const unsigned grid = (unsigned)((c->E + kApply32Threads - 1) / kApply32Threads);
-    k_apply32<NPE, MODEL><<<grid, kApply32Threads, 0, c->stream>>>(c->E, c->conn, c->mf_d, c->mf_c,
-                                                                   c->nqp, v, ye, done);
+    k_apply32<NPE, MODEL><<<grid, kApply32Threads, 0, c->stream>>>(
+        c->E, c->conn, c->mf_d, c->mf_c, c->nqp, (float)c->mat.bulk_modulus, v, ye, done);
 }
 
 // ye = K_e v_e per element in FP32 (graph-capturable: launches only)

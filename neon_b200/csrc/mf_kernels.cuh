@@ -22,11 +22,13 @@ __device__ __forceinline__ float det3f(const float* m) {
            m[2] * (m[3] * m[7] - m[4] * m[6]);
 }
 
-__device__ __forceinline__ void inv3f(const float* m, float* r) {
+// r = m^-1; returns det m
+__device__ __forceinline__ float inv3f(const float* m, float* r) {
     const float c00 = m[4] * m[8] - m[5] * m[7];
     const float c10 = m[7] * m[2] - m[8] * m[1];
     const float c20 = m[1] * m[5] - m[2] * m[4];
-    const float id = 1.0f / (c00 * m[0] + c10 * m[3] + c20 * m[6]);
+    const float det = c00 * m[0] + c10 * m[3] + c20 * m[6];
+    const float id = 1.0f / det;
     r[0] = c00 * id;
     r[1] = c10 * id;
     r[2] = c20 * id;
@@ -36,19 +38,29 @@ __device__ __forceinline__ void inv3f(const float* m, float* r) {
     r[6] = (m[3] * m[7] - m[4] * m[6]) * id;
     r[7] = (m[6] * m[1] - m[7] * m[0]) * id;
     r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+    return det;
 }
 
 // number of FP32 coefficients per quadrature point
 template <int MODEL>
 struct MfCoef {
     static constexpr int KC =
-        (MODEL == MODEL_J2) ? 9 : ((MODEL == MODEL_LE) ? 2 : (model_aniso(MODEL) ? 8 + 21 : 8));
+        (MODEL == MODEL_J2) ? 6 : ((MODEL == MODEL_LE) ? 2 : (model_aniso(MODEL) ? 8 + 21 : 8));
 };
 
 // Setup from the stored FP64 outputs of the last MODE_STORE pass (A.u = its displacement):
 //   md[e][3a+k]  = (float)(x_a - x_0)_k
-//   mc[c][q]     = s lam', s mu' | J2: s b, N (6) | finite strain: s sigma (6)
+//   mc[c][q]     = s lam', s mu' | finite strain: then s sigma (6)
 //                  | Langevin / non-affine microsphere: then s Da (21, packed upper triangle)
+//                  | J2: mu' (negated at a plastic point), m = sqrt(-b) N as its 11 22 23 13 12
+//                    components (N is deviatoric, so m_33 = -m_11 - m_22).  The J2 tangent is
+//                    lam' I(x)I + 2 mu' I + b N(x)N with lam' = K - 2 mu'/3, and b < 0 at a
+//                    plastic point (b = -6 G^2 sigma_y(ebar) / (q_trial (3G + H)) for the linear
+//                    hardening return map), so b N(x)N = -m(x)m.  The point weight s = w det J
+//                    comes from the element's own FP32 geometry at apply time.  Six numbers per
+//                    point instead of nine, one at an elastic point.  (Were b ever positive, the
+//                    operator would drop that term: the FP64 residual replacements still
+//                    converge, only more slowly.)
 //   de[a][e][i]  = element contribution to K_(3a+i, 3a+i) (the per-node planes of ye)
 template <int NPE, int MODEL>
 __global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restrict__ md,
@@ -103,16 +115,21 @@ __global__ void __launch_bounds__(64) k_mf_setup(ElementArgs A, float* __restric
         const double s = w * det3(Fc);
         const double lam = A.dpar[0 * n + q], mu = A.dpar[1 * n + q];
         double b = 0.0, N6[6] = {0, 0, 0, 0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0};
-        mc[0 * n + q] = (float)(s * lam);
-        mc[1 * n + q] = (float)(s * mu);
         if constexpr (kJ2) {
             b = A.dpar[2 * n + q];
-            mc[2 * n + q] = (float)(s * b);
 #pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                N6[c] = A.dpar[(3 + c) * n + q];
-                mc[(3 + c) * n + q] = (float)N6[c];
-            }
+            for (int c = 0; c < 6; ++c) N6[c] = A.dpar[(3 + c) * n + q];
+            const bool plastic = b != 0.0;
+            mc[0 * n + q] = plastic ? -(float)fmax(mu, 1e-30) : (float)mu;
+            const double sb = plastic ? sqrt(fmax(-b, 0.0)) : 0.0;
+            mc[1 * n + q] = (float)(sb * N6[0]);
+            mc[2 * n + q] = (float)(sb * N6[1]);
+            mc[3 * n + q] = (float)(sb * N6[3]);
+            mc[4 * n + q] = (float)(sb * N6[4]);
+            mc[5 * n + q] = (float)(sb * N6[5]);
+        } else {
+            mc[0 * n + q] = (float)(s * lam);
+            mc[1 * n + q] = (float)(s * mu);
         }
         if constexpr (kFinite) {
 #pragma unroll
@@ -192,15 +209,17 @@ __device__ __forceinline__ float dNf(int i) {
         return c_dNf_tet4[i];
 }
 
-// P = S J^-T at one point (J, Gx as defined above, in the same scaling)
+// P = S J^-T at one point (J, Gx as defined above, in the same scaling).  J2 only: kdet turns
+// det J into the point weight s (w times the determinant of the true Jacobian), Kb is the bulk
+// modulus.
 template <int MODEL>
 __device__ __forceinline__ void point_flux(const float* J, const float* Gx,
                                            const float* __restrict__ mc, long long nqp,
-                                           long long q, float* Pm) {
+                                           long long q, float kdet, float Kb, float* Pm) {
     constexpr bool kFinite = (MODEL == MODEL_NH || MODEL == MODEL_MS || model_aniso(MODEL));
     constexpr bool kJ2 = (MODEL == MODEL_J2);
     float Ji[9];
-    inv3f(J, Ji);
+    const float det = inv3f(J, Ji);
     float G[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -208,7 +227,17 @@ __device__ __forceinline__ void point_flux(const float* J, const float* Gx,
         for (int k = 0; k < 3; ++k)
             G[i * 3 + k] = Gx[i * 3 + 0] * Ji[0 * 3 + k] + Gx[i * 3 + 1] * Ji[1 * 3 + k] +
                            Gx[i * 3 + 2] * Ji[2 * 3 + k];
-    const float cl = mc[0 * nqp + q], cm = mc[1 * nqp + q];
+    float cl, cm, c0 = 0.0f, sw = 0.0f;
+    if constexpr (kJ2) {
+        c0 = mc[0 * nqp + q];
+        const float mu = fabsf(c0);
+        sw = det * kdet;
+        cm = sw * mu;
+        cl = sw * (Kb - (2.0f / 3.0f) * mu);
+    } else {
+        cl = mc[0 * nqp + q];
+        cm = mc[1 * nqp + q];
+    }
     const float ltr = cl * (G[0] + G[4] + G[8]);
     float S[9];
 #pragma unroll
@@ -217,19 +246,17 @@ __device__ __forceinline__ void point_flux(const float* J, const float* Gx,
         for (int k = 0; k < 3; ++k)
             S[i * 3 + k] = cm * (G[i * 3 + k] + G[k * 3 + i]) + (i == k ? ltr : 0.0f);
     if constexpr (kJ2) {
-        const float cb = mc[2 * nqp + q];
-        if (cb != 0.0f) {
-            float N6[6];
-#pragma unroll
-            for (int c = 0; c < 6; ++c) N6[c] = mc[(3 + c) * nqp + q];
-            const float bN = cb * (N6[0] * G[0] + N6[1] * G[4] + N6[2] * G[8] +
-                                   N6[3] * (G[5] + G[7]) + N6[4] * (G[2] + G[6]) +
-                                   N6[5] * (G[1] + G[3]));
-            // N symmetric (11 22 33 23 13 12)
-            S[0] += bN * N6[0]; S[4] += bN * N6[1]; S[8] += bN * N6[2];
-            S[5] += bN * N6[3]; S[7] += bN * N6[3];
-            S[2] += bN * N6[4]; S[6] += bN * N6[4];
-            S[1] += bN * N6[5]; S[3] += bN * N6[5];
+        if (c0 < 0.0f) {  // plastic point: S -= s (m:G) m
+            const float m0 = mc[1 * nqp + q], m1 = mc[2 * nqp + q], m3 = mc[3 * nqp + q],
+                        m4 = mc[4 * nqp + q], m5 = mc[5 * nqp + q];
+            const float m2 = -(m0 + m1);
+            const float bN = -sw * (m0 * G[0] + m1 * G[4] + m2 * G[8] + m3 * (G[5] + G[7]) +
+                                    m4 * (G[2] + G[6]) + m5 * (G[1] + G[3]));
+            // m symmetric (11 22 33 23 13 12)
+            S[0] += bN * m0; S[4] += bN * m1; S[8] += bN * m2;
+            S[5] += bN * m3; S[7] += bN * m3;
+            S[2] += bN * m4; S[6] += bN * m4;
+            S[1] += bN * m5; S[3] += bN * m5;
         }
     }
     if constexpr (model_aniso(MODEL)) {
@@ -300,7 +327,7 @@ __global__ void __launch_bounds__(kApply32Threads, (MODEL == MODEL_J2 || MODEL =
 k_apply32(int E, const int* __restrict__ conn,
                                                              const float* __restrict__ md,
                                                              const float* __restrict__ mc,
-                                                             long long nqp,
+                                                             long long nqp, float Kb,
                                                              const float* __restrict__ v,
                                                              float* __restrict__ ye,
                                                              const int* __restrict__ done) {
@@ -347,7 +374,7 @@ k_apply32(int E, const int* __restrict__ conn,
             float J[9], Gx[9], Pm[9];
             hex8_grad(Md, x, ee, z, J);
             hex8_grad(Mv, x, ee, z, Gx);
-            point_flux<MODEL>(J, Gx, mc, nqp, e * 8 + l, Pm);
+            point_flux<MODEL>(J, Gx, mc, nqp, e * 8 + l, 1.0f / 512.0f, Kb, Pm);
             const float ez = ee * z, xz = x * z, xe = x * ee;
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
@@ -401,7 +428,7 @@ k_apply32(int E, const int* __restrict__ conn,
                     }
                 }
             float Pm[9];
-            point_flux<MODEL>(J, Gx, mc, nqp, e * NQ + l, Pm);
+            point_flux<MODEL>(J, Gx, mc, nqp, e * NQ + l, 1.0f / 6.0f, Kb, Pm);
 #pragma unroll
             for (int a = 0; a < NPE; ++a) {
                 const float g0 = dNf<NPE>((l * NPE + a) * 3 + 0), g1 = dNf<NPE>((l * NPE + a) * 3 + 1),
