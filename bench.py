@@ -352,7 +352,7 @@ def main():
     ap.add_argument("--cg-iterations", type=int, default=200)
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--batch-delta", type=float, default=1e-3,
+    ap.add_argument("--batch-delta", type=float, default=1e-2,
                     help="reliable-update interval of the batched mixed path")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-c2", action="store_true")

@@ -514,7 +514,7 @@ class BatchedStaticMatrix:
     (per-element moduli), boundary tables, load stepping, Newton decisions and PCG.  All problems
     share one constitutive model and one set of solver options (those of the first problem)."""
 
-    def __init__(self, problems, precision=FP64, mixed_inner_tolerance=1e-4, use_graphs=True,
+    def __init__(self, problems, precision=FP64, mixed_inner_tolerance=1e-2, use_graphs=True,
                  autotune=True):
         self.problems = list(problems)
         self.layout = batch_layout(self.problems)

@@ -153,7 +153,8 @@ __global__ void __launch_bounds__(kThreads) k_b_spmv(Tables T, const int* __rest
                                                      const V* __restrict__ val,
                                                      const X* __restrict__ p, X* __restrict__ q,
                                                      const unsigned char* __restrict__ mask,
-                                                     Scalars S, double* part) {
+                                                     Scalars S, double* part,
+                                                     const float* __restrict__ dc) {
     const int inst = T.inst[blockIdx.x];
     if (S.done[inst]) return;
     constexpr int RPW = 32 / LPR;  // rows of a warp in flight
@@ -184,6 +185,7 @@ __global__ void __launch_bounds__(kThreads) k_b_spmv(Tables T, const int* __rest
         if (a < r1 && sl < 3) {
             const long long i = 3ll * a + sl;
             X y = sl == 0 ? y0 : (sl == 1 ? y1 : y2);
+            if (dc) y += (X)dc[i] * p[i];
             if (mask && mask[i]) y = (X)0;
             q[i] = y;
             dot[0] += (double)p[i] * (double)y;
@@ -374,6 +376,35 @@ __global__ void k_b_invdiag(const int* brp, const int* bcol, const V* val, int r
     }
 }
 
+// FP32 K with a compensated diagonal.  The tangent of any of these models is unchanged by a
+// rigid translation (f_int does not move when every node does), so in each row the entries of
+// one component sum to zero: K_(3a+r, 3a+r) = -sum_(b != a) K_(3a+r, 3b+r).  Rounding K to FP32
+// breaks that identity by about the rounding of the diagonal, which is the largest entry, and
+// the translation-like modes that give the small eigenvalues then see a relatively large
+// operator error.  dc restores it: dc = -(sum of the FP32 off-diagonal same-component entries,
+// in FP64) - (FP32 diagonal), added as dc p in the SpMV, so the operator's diagonal is the
+// compensated value and every row sums to zero again to FP64 rounding.  The Jacobi inverse uses
+// the same diagonal (1 where it is 0).
+__global__ void k_b_compdiag(const int* brp, const int* bcol, const float* val, int rows,
+                             float* dc, double* inv) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= rows) return;
+    double off[3] = {0.0, 0.0, 0.0}, d[3] = {0.0, 0.0, 0.0};
+    for (int k = brp[a]; k < brp[a + 1]; ++k) {
+        const float* blk = val + 9ll * k;
+        if (bcol[k] == a) {
+            for (int r = 0; r < 3; ++r) d[r] = (double)blk[4 * r];
+        } else {
+            for (int r = 0; r < 3; ++r) off[r] += (double)blk[4 * r];
+        }
+    }
+    for (int r = 0; r < 3; ++r) {
+        const double dd = -off[r];
+        dc[3ll * a + r] = (float)(dd - d[r]);
+        inv[3ll * a + r] = dd != 0.0 ? 1.0 / dd : 1.0;
+    }
+}
+
 template <typename X>
 __global__ void k_b_out(long long n, const X* x, double* out) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -429,7 +460,7 @@ unsigned vgrid(long long n) { return (unsigned)std::min<long long>((n + 255) / 2
 
 template <typename V, typename X>
 using SpmvFn = void (*)(Tables, const int*, const int*, const V*, const X*, X*,
-                        const unsigned char*, Scalars, double*);
+                        const unsigned char*, Scalars, double*, const float*);
 
 template <typename V, typename X>
 SpmvFn<V, X> spmv_variant(int lanes) {
@@ -458,6 +489,7 @@ struct BatchState {
     std::vector<int> h_done, h_iters, h_status;
     std::vector<double> h_norms;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    float* dcomp = nullptr;    // FP32 K mode: the compensated diagonal's correction (n)
 
     Tables tables() const { return Tables{row0, row1, inst, first, count}; }
     Scalars scalars() const {
@@ -487,7 +519,7 @@ void batch_release(BatchState* b) {
     for (cudaGraphExec_t g : b->graph)
         if (g) cudaGraphExecDestroy(g);
     void* ptrs[] = {b->row0, b->row1,    b->inst, b->first, b->count,  b->dbuf,
-                    b->ibuf, b->tickets, b->part, b->norms, b->flag_a, b->flag_b};
+                    b->ibuf, b->tickets, b->part, b->norms, b->flag_a, b->flag_b, b->dcomp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete b;
@@ -589,9 +621,11 @@ int batch_pcg_start(nb2_ctx* c, BatchState* b, int mode, const double* rhs, doub
     if (mode == kModeK64)
         k_b_invdiag<double, double><<<g, 256, 0, c->stream>>>(c->brp, c->bcol, c->K64, c->N,
                                                               c->cg_inv);
-    else
-        k_b_invdiag<float, double><<<g, 256, 0, c->stream>>>(c->brp, c->bcol, c->K32, c->N,
-                                                             c->cg_inv);
+    else {
+        if (!b->dcomp) NB2_CUDA(c, cudaMalloc(&b->dcomp, sizeof(float) * c->n));
+        k_b_compdiag<<<g, 256, 0, c->stream>>>(c->brp, c->bcol, c->K32, c->N, b->dcomp,
+                                               c->cg_inv);
+    }
     NB2_CUDA(c, cudaMemcpyAsync(S.maxit, maxit.data(), sizeof(int) * b->ninst,
                                 cudaMemcpyHostToDevice, c->stream));
     k_b_init<double><<<b->nchunks, kThreads, 0, c->stream>>>(T, rhs, c->cg_x, c->cg_r, c->cg_p,
@@ -611,10 +645,10 @@ int batch_pcg_iterate(nb2_ctx* c, BatchState* b, int mode, int most, bool graphs
         for (int it = 0; it < kBatchChunk; ++it) {
             if (mode == kModeK64)
                 spmv64<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K64, c->cg_p,
-                                                       c->cg_q, c->mask, S, b->part);
+                                                       c->cg_q, c->mask, S, b->part, nullptr);
             else
                 spmv3264<<<nb, kThreads, 0, c->stream>>>(T, c->brp, c->bcol, c->K32, c->cg_p,
-                                                         c->cg_q, c->mask, S, b->part);
+                                                         c->cg_q, c->mask, S, b->part, b->dcomp);
             k_b_xr<double><<<nb, kThreads, 0, c->stream>>>(T, c->cg_x, c->cg_r, c->cg_p, c->cg_q,
                                                            c->cg_inv, S, b->part);
             k_b_p<double><<<nb, kThreads, 0, c->stream>>>(T, c->cg_p, c->cg_r, c->cg_inv, S);
@@ -1177,16 +1211,18 @@ extern "C" int nb2_batch_autotune(nb2_ctx* c, int32_t num_instances, const int32
         if (st) break;
         Scalars S = b->scalars();
         S.timing = 1;
+        if (!f64 && cudaMalloc(&b->dcomp, sizeof(float) * c->n) == cudaSuccess)
+            cudaMemsetAsync(b->dcomp, 0, sizeof(float) * c->n, c->stream);  // timed like the solve's
         for (int L : lanes) {
             auto sweep = [&]() {
                 if (f64)
                     spmv_variant<double, double>(L)<<<b->nchunks, kThreads, 0, c->stream>>>(
                         b->tables(), c->brp, c->bcol, c->K64, c->cg_p, c->cg_q, c->mask, S,
-                        b->part);
+                        b->part, nullptr);
                 else  // the batched mixed mode: FP32 K, FP64 vectors
                     spmv_variant<float, double>(L)<<<b->nchunks, kThreads, 0, c->stream>>>(
                         b->tables(), c->brp, c->bcol, c->K32, c->cg_p, c->cg_q, c->mask, S,
-                        b->part);
+                        b->part, b->dcomp);
             };
             sweep();
             cudaEventRecord(e0, c->stream);
