@@ -37,9 +37,8 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
-    deps = [os.path.join(CSRC, s) for s in SOURCES] + [
-        os.path.join(CSRC, "nb2_internal.cuh"), os.path.join(CSRC, "host_driver.hpp"),
-        os.path.join(CSRC, "element_kernel.cuh"),
+    headers = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h")))
+    deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, h) for h in headers] + [
         os.path.join(ROOT, "include", "neon_b200.h"),
         os.path.join(ROOT, "include", "neon_b200_probe.h")]
     if not force and not _stale(LIB, deps):

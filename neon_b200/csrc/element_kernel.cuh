@@ -32,8 +32,14 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
     constexpr bool kStiff = (MODE & MODE_STIFFNESS) != 0;
     constexpr bool kForce = (MODE & MODE_FORCE) != 0;
     constexpr bool kStore = (MODE & MODE_STORE) != 0;
-    constexpr int LS = NQ * NPE * 3 + 2;           // per-element stride of L (padded)
-    constexpr int NS = kJ2 ? NQ * 6 + 2 : (kAniso ? NQ * 21 + 2 : 1);  // N or s Da
+    // L per element: one row of NPE * 3 values per point.  hex8 pads each row to 25 doubles and
+    // the element to 200: the 32 lanes of a warp (4 elements x 8 points) then store a row entry
+    // in 2 shared-memory wavefronts instead of 8 (and the phase-2 loads stay at 4).
+    constexpr int QS = (NPE == 8) ? NPE * 3 + 1 : NPE * 3;
+    constexpr int LS = (NPE == 8) ? NQ * QS : NQ * QS + 2;
+    // N (J2, 6 per point; an odd element stride puts the two elements of a half-warp on
+    // different banks) or s Da
+    constexpr int NS = kJ2 ? NQ * 6 + 1 : (kAniso ? NQ * 21 + 2 : 1);
     constexpr int GS = kFinite ? NQ * NPE * 3 + 1 : 1;  // g = s sigma L
     constexpr int NG = (NPE + G - 1) / G;          // nodes per lane
     // hex8 FP64 blocks on the FP64 mma.sync path (the anisotropic microsphere tangent keeps the
@@ -231,7 +237,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                 if (active) {
                     if constexpr (kStiff) {
 #pragma unroll
-                        for (int k = 0; k < 3; ++k) sL[le][l * NPE * 3 + 3 * a + k] = (Real)La[k];
+                        for (int k = 0; k < 3; ++k) sL[le][l * QS + 3 * a + k] = (Real)La[k];
                     }
                     if constexpr (kFinite && kStiff) {
 #pragma unroll
@@ -351,7 +357,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
             for (int st = 0; st < 2; ++st) {
                 const int q = t + 4 * st;
 #pragma unroll
-                for (int k = 0; k < 3; ++k) Lq[st][k] = (double)sL[le2][q * NPE * 3 + 3 * g + k];
+                for (int k = 0; k < 3; ++k) Lq[st][k] = (double)sL[le2][q * QS + 3 * g + k];
                 cl[st] = (double)sC[le2][q][0];
                 cm[st] = (double)sC[le2][q][1];
                 cb[st] = (double)sC[le2][q][2];
@@ -460,7 +466,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
 #pragma unroll
                 for (int i = 0; i < 9; ++i) acc[j][i] = (Real)0;
             for (int l = 0; l < NQ; ++l) {
-                const Real* Ll = &sL[le][l * NPE * 3];
+                const Real* Ll = &sL[le][l * QS];
                 const Real cl = sC[le][l][0], cm = sC[le][l][1], cb = sC[le][l][2];
                 Real Nq[6];
                 if constexpr (kJ2) {
