@@ -75,8 +75,10 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
     const long long e = element_at(A, (long long)blockIdx.x * EPC + le);
     const bool valid = element_enabled(A, e);
 
-    for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
-        sdN[i / (NPE * 3)][(i % (NPE * 3)) / 3][i % 3] = (NPE == 8) ? c_dN_hex8[i] : c_dN_tet4[i];
+    if constexpr (NPE != 8) {  // hex8 forms its derivatives in registers (hex8_dN)
+        for (int i = tid; i < NQ * NPE * 3; i += blockDim.x)
+            sdN[i / (NPE * 3)][(i % (NPE * 3)) / 3][i % 3] = c_dN_tet4[i];
+    }
 
     // phase 0
     int node[NG];
@@ -103,6 +105,7 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
     for (int j = 0; j < NG; ++j) fown[j][0] = fown[j][1] = fown[j][2] = 0.0;
     {
         const int l = lane;
+        [[maybe_unused]] const Hex8Point hp = hex8_point(l);
         const bool active = valid && l < NQ;
         QpOut o;
         o.lam = o.mu = o.b = 0.0;
@@ -131,7 +134,11 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
                     const double xi = sx[le][a][i], Xi = sX[le][a][i], di = xi - Xi;
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
-                        const double d = sdN[l][a][k];
+                        double d;
+                        if constexpr (NPE == 8)
+                            d = hex8_dN(hp, a, k);
+                        else
+                            d = sdN[l][a][k];
                         if constexpr (kCon) {
                             F0[i * 3 + k] += Xi * d;
                             U[i * 3 + k] += di * d;
@@ -225,10 +232,17 @@ __global__ void __launch_bounds__(64, (MODEL == MODEL_J2) ? 8 : (model_aniso(MOD
             auto node_terms = [&](int a, double (&gv)[3]) {
                 double La[3] = {0.0, 0.0, 0.0};
                 if (active) {
+                    double dn[3];
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) {
+                        if constexpr (NPE == 8)
+                            dn[m] = hex8_dN(hp, a, m);
+                        else
+                            dn[m] = sdN[l][a][m];
+                    }
 #pragma unroll
                     for (int k = 0; k < 3; ++k)
-                        La[k] = sdN[l][a][0] * Ji[0 * 3 + k] + sdN[l][a][1] * Ji[1 * 3 + k] +
-                                sdN[l][a][2] * Ji[2 * 3 + k];
+                        La[k] = dn[0] * Ji[0 * 3 + k] + dn[1] * Ji[1 * 3 + k] + dn[2] * Ji[2 * 3 + k];
                 }
                 // sigma symmetric: 11 22 33 23 13 12
                 gv[0] = s * (o.sig[0] * La[0] + o.sig[5] * La[1] + o.sig[4] * La[2]);

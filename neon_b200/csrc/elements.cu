@@ -43,6 +43,7 @@ namespace nb2 {
 
 __constant__ double c_dN_hex8[8 * 8 * 3];
 __constant__ double c_w_hex8[8];
+__constant__ double c_hex8_g;  // 1/sqrt(3) as the host computed it for c_dN_hex8
 __constant__ double c_dN_tet4[4 * 3];
 __constant__ float c_dNf_hex8[8 * 8 * 3];  // FP32 copies for the matrix-free FP32 operator
 __constant__ float c_dNf_tet4[4 * 3];
@@ -537,6 +538,41 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(d[0]), "+d"(d[1])
                  : "d"(a), "d"(b));
+}
+
+// hexahedron8 shape-function derivatives at one point of the 8-point rule, in registers: the
+// point's factors 1 + s x (s = -1, +1 for each reference coordinate x) are formed once, and each
+// derivative is the product the host table c_dN_hex8 evaluates, in its order, so the values are
+// the same bits (hexahedron.cpp:10-67).  The fused element kernel uses it instead of a shared
+// table, whose broadcast reads cost two shared-memory wavefronts per 64-bit load.
+struct Hex8Point {
+    double f[3][2];  // [reference coordinate][s = -1, +1]
+};
+
+__device__ __forceinline__ Hex8Point hex8_point(int l) {
+    const double g = c_hex8_g;
+    const double x = ((l == 1) || (l == 2) || (l == 5) || (l == 6)) ? g : -g;
+    const double e = ((l == 2) || (l == 3) || (l == 6) || (l == 7)) ? g : -g;
+    const double z = (l >= 4) ? g : -g;
+    Hex8Point P;
+    P.f[0][0] = 1.0 + (-1.0) * x;
+    P.f[0][1] = 1.0 + 1.0 * x;
+    P.f[1][0] = 1.0 + (-1.0) * e;
+    P.f[1][1] = 1.0 + 1.0 * e;
+    P.f[2][0] = 1.0 + (-1.0) * z;
+    P.f[2][1] = 1.0 + 1.0 * z;
+    return P;
+}
+
+// dN_a / dxi_k (a, k known at compile time once the callers' loops unroll)
+__device__ __forceinline__ double hex8_dN(const Hex8Point& P, int a, int k) {
+    const int sx = ((a == 1) || (a == 2) || (a == 5) || (a == 6)) ? 1 : 0;
+    const int se = ((a == 2) || (a == 3) || (a == 6) || (a == 7)) ? 1 : 0;
+    const int sz = (a >= 4) ? 1 : 0;
+    const double xa = sx ? 1.0 : -1.0, ea = se ? 1.0 : -1.0, za = sz ? 1.0 : -1.0;
+    if (k == 0) return 1.0 / 8.0 * xa * P.f[1][se] * P.f[2][sz];
+    if (k == 1) return 1.0 / 8.0 * P.f[0][sx] * ea * P.f[2][sz];
+    return 1.0 / 8.0 * P.f[0][sx] * P.f[1][se] * za;
 }
 
 #include "element_kernel.cuh"
@@ -1137,6 +1173,7 @@ static int upload_tables(nb2_ctx* c) {
     for (int i = 0; i < 33; ++i) sw[21 + i] = i < 3 ? v1 : (i < 9 ? v2 : (i < 21 ? v3 : v4));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_dN_hex8, dN, sizeof dN));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_w_hex8, w, sizeof w));
+    NB2_CUDA(c, cudaMemcpyToSymbol(c_hex8_g, &g, sizeof g));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_dN_tet4, dNt, sizeof dNt));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_sphere_r, rr, sizeof rr));
     NB2_CUDA(c, cudaMemcpyToSymbol(c_sphere_w, sw, sizeof sw));
