@@ -879,10 +879,10 @@ struct BatchNewton {
     }
 
     // Per-instance mixed precision with reliable updates (the batched counterpart of
-    // pcg_reliable_mixed): iterations on the FP32 K32 with FP64 vectors -- on these nearly
-    // incompressible tet4 systems FP32 vector recurrences cost 50-60% more iterations, while K32
-    // carries most of the bytes -- and when every instance has paused (its recursive residual
-    // fell by delta) or finished, the paused ones get the true residual b - K x with the FP64
+    // pcg_reliable_mixed): iterations on the FP32 K32 (its diagonal compensated, k_b_compdiag)
+    // with FP64 vectors -- K32 carries most of the bytes, and FP32 vector recurrences cost more
+    // iterations than they save on these nearly incompressible tet4 systems -- and when every
+    // instance has paused (its recursive residual fell by delta) or finished, the paused ones get the true residual b - K x with the FP64
     // tangent (matrix-free, stored coefficients, only their elements) and continue with it,
     // keeping their search directions.
     int solve_mixed(const std::vector<int>& solving, std::vector<int>& its, std::vector<int>& st) {
