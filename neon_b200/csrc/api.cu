@@ -1012,7 +1012,11 @@ extern "C" int nb2_static_solve(nb2_ctx* c, const nb2_solver_options* options,
         if (!(nw.o.mixed_inner_tolerance > 0)) nw.o.mixed_inner_tolerance = 1e-4;
     } else {
         NB2_TRY(ensure_k64(c));
+        // the second K buffer the element passes zero in the background
+        if (!c->e_inst) NB2_TRY(ensure_k64_alt(c));
     }
+    // the element colouring of the Newton driver's (bit-reproducible) hex8 element passes
+    if (c->npe == 8 && !c->e_inst) NB2_TRY(ensure_colouring(c));
     auto t0 = std::chrono::steady_clock::now();
     nw.use_relative_norm = options->absolute_tolerance == 0;
     NB2_CUDA(c, cudaEventCreate(&nw.ev0));
