@@ -252,3 +252,39 @@ def test_non_adaptive_and_absolute_tolerance():
     assert (o.initial, o.minimum, o.maximum, o.adaptive) == (0.25, 0.25, 0.25, False)
     assert o.absolute_tolerance
     assert (o.cg_tolerance, o.cg_maximum_iterations) == (1e-5, 2000)
+
+
+def test_split_groups_are_joined(tmp_path):
+    """A part (and a boundary) stored as several groups of one name, as gmsh writes physical
+    groups made of several entities: basic_mesh::meshes returns them all, and both readers join
+    them into one element list and one set of boundary nodes."""
+    deck, mesh_file = loaded_block_deck("hex8", "neohooke")
+    groups = []
+    for g in mesh_file["Elements"]:
+        conn = g["NodalConnectivity"]
+        half = len(conn) // 2
+        groups.append(dict(g, NodalConnectivity=conn[:half]))
+        groups.append(dict(g, NodalConnectivity=conn[half:]))
+    split = dict(mesh_file, Elements=groups)
+    whole, _ = _check_same_parse(tmp_path, deck, mesh_file)
+    parts, _ = _check_same_parse(tmp_path, deck, split)
+    assert np.array_equal(parts.mesh.conn, whole.mesh.conn)
+    _same_tables(whole.dirichlet, [{"dofs": t.dofs, "times": t.times, "values": t.values}
+                                   for t in parts.dirichlet])
+    for a, b in zip(whole.loads, parts.loads):
+        assert np.array_equal(a.faces, b.faces) if a.faces is not None else b.faces is None
+
+
+def test_mixed_element_types_in_a_group_are_refused(tmp_path):
+    """One group name holding quadrilateral and triangle faces: neither reader runs it (one
+    element type per group is on this path)."""
+    deck, mesh_file = loaded_block_deck("hex8", "neohooke")
+    bad = copy.deepcopy(mesh_file)
+    top = next(g for g in bad["Elements"] if g["Name"] == "top")
+    tri = [q[:3] for q in top["NodalConnectivity"][:2]]
+    bad["Elements"].append({"Name": "top", "Type": 2, "NodalConnectivity": tri})
+    with pytest.raises(NotImplementedError, match="mixes element types"):
+        D.problem_from_deck(deck, bad)
+    out = run_adapter_driver(tmp_path, deck, bad, "--parse-only")
+    if out is not None:
+        assert out["error"] == "domain_error" and "mixes element types" in out["what"]
